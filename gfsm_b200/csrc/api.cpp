@@ -1,0 +1,335 @@
+// api.cpp -- the C ABI (include/gfsm.h) over the host parser/planner, the
+// device CCSR builder and the matching engine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "engine.h"
+#include "gfsm_internal.h"
+
+using namespace gfsm;
+
+namespace {
+
+uint64_t env_u64(const char *name, uint64_t dflt) {
+    const char *s = getenv(name);
+    if (!s || !*s) return dflt;
+    char *end = nullptr;
+    double v = strtod(s, &end);
+    if (end == s || v < 0) return dflt;
+    return (uint64_t)v;
+}
+
+gfsm_status set_err(gfsm_ctx *ctx, gfsm_status rc, const std::string &msg) {
+    if (ctx && rc != GFSM_OK) ctx->last_error = msg.empty() ? gfsm_status_str(rc) : msg;
+    return rc;
+}
+
+Engine *ctx_engine(gfsm_ctx *ctx, const DeviceGraph &g, gfsm_status &rc, std::string &err) {
+    Engine *e = static_cast<Engine *>(ctx->engine);
+    if (!e) {
+        e = new (std::nothrow) Engine();
+        if (!e) { rc = GFSM_ERR_NOMEM; return nullptr; }
+        rc = e->init(ctx->device, 0, ctx->lim.max_scan_size, err);
+        if (rc != GFSM_OK) { delete e; return nullptr; }
+        ctx->engine = e;
+    }
+    // MEMLIMIT covers the data graph, the engine's fixed buffers and the arena.
+    const uint64_t used = g.bytes + e->small_bytes;
+    uint64_t cap = ctx->lim.mem_limit > used ? ctx->lim.mem_limit - used : 0;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        uint64_t avail = (uint64_t)free_b + e->arena_bytes;
+        avail = avail > (1ull << 30) ? avail - (1ull << 30) : avail / 2;
+        cap = std::min(cap, avail);
+    }
+    if (e->arena && e->arena_bytes > cap) {
+        cudaFree(e->arena);
+        e->arena = nullptr;
+        e->arena_bytes = 0;
+    }
+    e->arena_cap = cap;
+    rc = GFSM_OK;
+    return e;
+}
+
+gfsm_status ensure_device(gfsm_ctx *ctx, gfsm_graph *g) {
+    if (g->dev) return GFSM_OK;
+    if (ctx->device < 0) return set_err(ctx, GFSM_ERR_NO_EXTENSION, "host-only context: no CUDA device bound");
+    auto *dg = new (std::nothrow) DeviceGraph();
+    if (!dg) return GFSM_ERR_NOMEM;
+    std::string err;
+    gfsm_status rc = build_device_graph(g->h, ctx->device, g->vl_mode, *dg, err);
+    if (rc != GFSM_OK) {
+        delete dg;
+        return set_err(ctx, rc, "device CCSR build: " + err);
+    }
+    g->dev = dg;
+    return GFSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gfsm_limits_default(gfsm_limits *lim) {
+    if (!lim) return;
+    lim->ccsr_rel_size = (uint32_t)env_u64("GFSM_CCSRRELSIZE", kCCSRRelSize);
+    lim->max_soln_size = env_u64("GFSM_MAXSOLNSIZE", kMaxSolnSize);
+    lim->max_scan_size = env_u64("GFSM_MAXSCANSIZE", kMaxScanSize);
+    lim->upper_mem_limit = env_u64("GFSM_UPPERMEMLIMIT", kUpperMemLimit);
+    lim->mem_limit = env_u64("GFSM_MEMLIMIT", kMemLimit);
+    lim->vertex_labels = (int32_t)env_u64("GFSM_VERTEX_LABELS", 0);
+    lim->degree_filter = (int32_t)env_u64("GFSM_DEGREE_FILTER", 1);
+}
+
+const char *gfsm_status_str(gfsm_status s) {
+    switch (s) {
+    case GFSM_OK: return "ok";
+    case GFSM_ERR_QUERY: return "query cannot be planned (disconnected or unsupported)";
+    case GFSM_ERR_MISSING_FILE: return "missing file";
+    case GFSM_ERR_INVALID_DATA: return "invalid graph data";
+    case GFSM_ERR_MISSING_DATA: return "missing graph data";
+    case GFSM_ERR_ARG: return "invalid argument";
+    case GFSM_ERR_CUDA: return "CUDA error";
+    case GFSM_ERR_NOMEM: return "MEMLIMIT too small";
+    case GFSM_ERR_TOO_LARGE: return "graph or query too large";
+    case GFSM_ERR_DEVICE_WAIT: return "bounded device wait ran out";
+    case GFSM_ERR_NO_EXTENSION: return "no CUDA device";
+    case GFSM_ERR_BUSY: return "queue full";
+    case GFSM_ERR_STOPPED: return "server stopped";
+    }
+    return "unknown status";
+}
+
+const char *gfsm_last_error(gfsm_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+gfsm_status gfsm_init(gfsm_ctx **out, const gfsm_limits *lim, int device) {
+    if (!out) return GFSM_ERR_ARG;
+    *out = nullptr;
+    gfsm_limits l;
+    if (lim) l = *lim;
+    else gfsm_limits_default(&l);
+    if (l.ccsr_rel_size < 1 || l.ccsr_rel_size > 8) return GFSM_ERR_ARG;
+    if (l.mem_limit > l.upper_mem_limit) return GFSM_ERR_ARG;
+    if (l.max_soln_size < 1024 || l.max_scan_size < 1024) return GFSM_ERR_ARG;
+    if (device == -1) {  // host-only context: parsing and planning, no matching
+        auto *ctx = new (std::nothrow) gfsm_ctx();
+        if (!ctx) return GFSM_ERR_NOMEM;
+        ctx->lim = l;
+        ctx->device = -1;
+        *out = ctx;
+        return GFSM_OK;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return GFSM_ERR_NO_EXTENSION;
+    }
+    if (device < 0 || device >= n) return GFSM_ERR_ARG;
+    auto *ctx = new (std::nothrow) gfsm_ctx();
+    if (!ctx) return GFSM_ERR_NOMEM;
+    ctx->lim = l;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return GFSM_ERR_CUDA;
+    }
+    *out = ctx;
+    return GFSM_OK;
+}
+
+void gfsm_destroy(gfsm_ctx *ctx) {
+    if (!ctx) return;
+    delete static_cast<Engine *>(ctx->engine);
+    delete ctx;
+}
+
+gfsm_status gfsm_graph_load_buffer(gfsm_ctx *ctx, const char *buf, uint64_t len, gfsm_graph **out) {
+    if (!ctx || !out || (!buf && len)) return GFSM_ERR_ARG;
+    *out = nullptr;
+    auto g = std::make_unique<gfsm_graph>();
+    g->ctx = ctx;
+    g->rel_bits = ctx->lim.ccsr_rel_size;
+    g->vl_mode = ctx->lim.vertex_labels != 0;
+    gfsm_status rc = parse_text(buf, len, g->rel_bits, g->h);
+    if (rc != GFSM_OK) return set_err(ctx, rc, "");
+    *out = g.release();
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_graph_load_text(gfsm_ctx *ctx, const char *path, gfsm_graph **out) {
+    if (!ctx || !path || !out) return GFSM_ERR_ARG;
+    *out = nullptr;
+    std::string text;
+    gfsm_status rc = read_file(path, text);
+    if (rc != GFSM_OK) return set_err(ctx, rc, std::string("missing file ") + path);
+    return gfsm_graph_load_buffer(ctx, text.data(), text.size(), out);
+}
+
+gfsm_status gfsm_graph_from_edges(gfsm_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                                  const uint32_t *elabel, const uint32_t *vlabel, gfsm_graph **out) {
+    if (!ctx || !out || (m && (!src || !dst))) return GFSM_ERR_ARG;
+    *out = nullptr;
+    if (m >= (1ull << 32)) return GFSM_ERR_TOO_LARGE;
+    auto g = std::make_unique<gfsm_graph>();
+    g->ctx = ctx;
+    g->rel_bits = ctx->lim.ccsr_rel_size;
+    g->vl_mode = ctx->lim.vertex_labels != 0;
+    HostGraph &h = g->h;
+    h.n = n;
+    h.src.assign(src, src + m);
+    h.dst.assign(dst, dst + m);
+    h.lab.resize(m);
+    const uint32_t vb = 32u - g->rel_bits;
+    for (uint64_t i = 0; i < m; ++i) {
+        if (src[i] >= n || dst[i] >= n) return set_err(ctx, GFSM_ERR_INVALID_DATA, "edge endpoint out of range");
+        const uint32_t l = elabel ? elabel[i] : 1u;
+        h.lab[i] = (uint8_t)(((uint32_t)(l << vb)) >> vb);
+    }
+    h.vlabel.assign(n, 0);
+    if (vlabel) std::memcpy(h.vlabel.data(), vlabel, (uint64_t)n * 4);
+    *out = g.release();
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_graph_to_device(gfsm_ctx *ctx, gfsm_graph *g) {
+    if (!ctx || !g) return GFSM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return ensure_device(ctx, g);
+}
+
+gfsm_status gfsm_graph_info_get(const gfsm_graph *g, gfsm_graph_info *info) {
+    if (!g || !info) return GFSM_ERR_ARG;
+    std::memset(info, 0, sizeof(*info));
+    info->n = g->h.n;
+    info->m = g->h.src.size();
+    if (g->dev) {
+        const DeviceGraph &d = *g->dev;
+        info->rows = d.rows;
+        info->max_degree = d.max_degree;
+        info->symmetric = d.symmetric;
+        info->multi_edges = d.multi;
+        info->n_edge_labels = d.n_edge_labels;
+        info->on_device = 1;
+        info->device_bytes = d.bytes;
+    } else {
+        std::vector<uint32_t> deg(g->h.n, 0);
+        for (uint32_t s : g->h.src) deg[s]++;
+        for (uint32_t x : deg) {
+            info->rows += x ? 1 : 0;
+            info->max_degree = std::max(info->max_degree, x);
+        }
+    }
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_graph_download(gfsm_ctx *ctx, const gfsm_graph *g, uint32_t *rowptr, uint32_t *adj, uint8_t *elab,
+                                uint32_t *order) {
+    if (!ctx || !g) return GFSM_ERR_ARG;
+    if (!g->dev) return GFSM_ERR_ARG;
+    const DeviceGraph &d = *g->dev;
+    cudaSetDevice(d.device);
+    if (rowptr) std::memcpy(rowptr, d.h_rowptr.data(), ((uint64_t)d.n + 1) * 4);
+    if (order) std::memcpy(order, d.h_order.data(), (uint64_t)d.n * 4);
+    if (adj && d.m && cudaMemcpy(adj, d.adj, d.m * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return GFSM_ERR_CUDA;
+    if (elab && d.m) {
+        if (d.elab) {
+            if (cudaMemcpy(elab, d.elab, d.m, cudaMemcpyDeviceToHost) != cudaSuccess) return GFSM_ERR_CUDA;
+        } else {
+            std::memset(elab, (int)d.single_label, d.m);
+        }
+    }
+    return GFSM_OK;
+}
+
+void gfsm_graph_destroy(gfsm_graph *g) {
+    if (!g) return;
+    if (g->dev) {
+        cudaSetDevice(g->dev->device);
+        free_device_graph(*g->dev);
+        delete g->dev;
+    }
+    delete g;
+}
+
+gfsm_status gfsm_query_prepare(gfsm_ctx *ctx, const gfsm_graph *q, gfsm_plan **out) {
+    if (!ctx || !q || !out) return GFSM_ERR_ARG;
+    *out = nullptr;
+    auto p = std::make_unique<gfsm_plan>();
+    gfsm_status rc = plan_query(q->h, q->rel_bits, p->p);
+    if (rc != GFSM_OK) return set_err(ctx, rc, "");
+    *out = p.release();
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_plan_tables(const gfsm_plan *p, uint32_t *k, uint32_t *max_valency, uint32_t *order,
+                             uint32_t *header, uint32_t *reqs) {
+    if (!p) return GFSM_ERR_ARG;
+    const Plan &x = p->p;
+    if (k) *k = x.k;
+    if (max_valency) *max_valency = x.max_valency;
+    if (order) std::copy(x.order.begin(), x.order.end(), order);
+    if (header) std::copy(x.header.begin(), x.header.end(), header);
+    if (reqs) {
+        // relation fields in the reference's packed form: label << CCSRVertSize
+        const uint32_t vb = 32u - x.rel_bits;
+        for (size_t i = 0; i < x.reqs.size(); ++i) reqs[i] = (i & 1) ? (x.reqs[i] << vb) : x.reqs[i];
+    }
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_plan_columns(const gfsm_plan *p, uint32_t *qvid) {
+    if (!p || !qvid) return GFSM_ERR_ARG;
+    std::copy(p->p.qvid.begin(), p->p.qvid.end(), qvid);
+    return GFSM_OK;
+}
+
+void gfsm_plan_destroy(gfsm_plan *p) { delete p; }
+
+gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq, const gfsm_graph *data,
+                             uint64_t *counts, gfsm_stats *stats) {
+    if (!ctx || !data || nq < 0 || (nq && (!plans || !counts))) return GFSM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    gfsm_status rc = ensure_device(ctx, const_cast<gfsm_graph *>(data));
+    if (rc != GFSM_OK) return rc;
+    std::string err;
+    Engine *e = ctx_engine(ctx, *data->dev, rc, err);
+    if (!e) return set_err(ctx, rc, err);
+    std::vector<const Plan *> ps(nq);
+    for (int i = 0; i < nq; ++i) {
+        if (!plans[i]) return GFSM_ERR_ARG;
+        ps[i] = &plans[i]->p;
+    }
+    rc = e->run(ps, *data->dev, ctx->lim, counts, stats, nullptr, 0, nullptr, err);
+    return set_err(ctx, rc, err);
+}
+
+gfsm_status gfsm_match_count(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data, uint64_t *count,
+                             gfsm_stats *stats) {
+    if (!plan || !count) return GFSM_ERR_ARG;
+    return gfsm_batch_count(ctx, &plan, 1, data, count, stats);
+}
+
+gfsm_status gfsm_match_mappings(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data, uint32_t *rows,
+                                uint64_t max_rows, uint64_t *n_rows, uint64_t *count, gfsm_stats *stats) {
+    if (!ctx || !plan || !data || !count || (max_rows && !rows)) return GFSM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    gfsm_status rc = ensure_device(ctx, const_cast<gfsm_graph *>(data));
+    if (rc != GFSM_OK) return rc;
+    std::string err;
+    Engine *e = ctx_engine(ctx, *data->dev, rc, err);
+    if (!e) return set_err(ctx, rc, err);
+    std::vector<const Plan *> ps{&plan->p};
+    uint64_t c = 0;
+    rc = e->run(ps, *data->dev, ctx->lim, &c, stats, rows, max_rows, n_rows, err);
+    *count = c;
+    return set_err(ctx, rc, err);
+}
+
+}  // extern "C"

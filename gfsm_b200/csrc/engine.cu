@@ -1,0 +1,778 @@
+// engine.cu -- the FFS level expansion on sm_100a (the hot path).
+//
+// Reference: HnGPU.cu:455-669 hnSolve drives, per level, hnGen (:114-185:
+// copy the anchor's row as candidates), hnCheck (:190-262: injectivity +
+// requirement rows), two CUB scans (:339-349) and hnRemove (:309-334:
+// compaction), with CDP launches and device-side syncs.
+//
+// Here one kernel, k_step, does a whole level step over a range of the
+// candidate space:
+//   * candidate space = for every parent partial mapping, the part of its
+//     anchor's row that passes the degree/label window of the new query
+//     vertex (rows are sorted by a degree-descending, label-grouped id, so
+//     the window is one contiguous slice found by two binary searches when
+//     the parent was produced);
+//   * tiles of 1024 candidates (256 threads x 4), so hub rows are split across
+//     tiles and every thread does the same amount of row work -- the load
+//     balance the reference's thread-per-parent hnGen lacks;
+//   * per candidate: injectivity against the parent tuple, the anchor's edge
+//     label, and a binary search in each other backward neighbour's row for
+//     the remaining requirements;
+//   * survivors are ranked with __ballot_sync/__popc, the tile's output
+//     offset (child count and next-level candidate count) comes from a
+//     decoupled look-back over tiles taken in launch order (bounded waits);
+//   * children are written as full tuples (SoA columns) together with their
+//     own next-level candidate slice, so the next step needs no scan, no
+//     pointer chasing up a forest, and no separate compaction;
+//   * at the last query vertex nothing is written: survivors are counted.
+// The host drives the steps depth-first over candidate chunks so that the
+// frontier never exceeds MEMLIMIT (the reference restarts at 2x memory).
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+
+namespace gfsm {
+
+namespace {
+
+constexpr int T = 256;
+constexpr int CPT = 4;
+constexpr int TILE = T * CPT;
+constexpr int WIN = TILE + 2;
+constexpr int NWARP = T / 32;
+constexpr uint32_t FLAG_AGG = 1, FLAG_INC = 2;
+constexpr uint32_t SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long status_word(uint32_t epoch, uint32_t flag, uint32_t cnt) {
+    return ((unsigned long long)epoch << 34) | ((unsigned long long)flag << 32) | cnt;
+}
+
+// First index in a[0, n) whose value is >= key (branch-free halving).
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
+    if (n == 0) return 0;
+    const uint32_t *base = a;
+    while (n > 1) {
+        uint32_t half = n >> 1;
+        base = (__ldg(base + half) < key) ? base + half : base;
+        n -= half;
+    }
+    return (uint32_t)(base - a) + (__ldg(base) < key ? 1u : 0u);
+}
+
+struct GraphView {
+    const uint32_t *__restrict__ rowptr;
+    const uint32_t *__restrict__ adj;
+    const uint8_t *__restrict__ elab;
+    const uint32_t *__restrict__ order;
+    uint32_t single_label;
+    uint32_t n;
+};
+
+// reqExists (HnGPU.cu:34-52) as a binary search: does u's row hold (v, lab)?
+__device__ __forceinline__ bool has_edge(const GraphView &g, uint32_t u, uint32_t v, uint32_t lab) {
+    const uint32_t rs = __ldg(g.rowptr + u), re = __ldg(g.rowptr + u + 1);
+    if (!g.elab && lab != g.single_label) return false;
+    uint32_t p = rs + lower_bound_u32(g.adj + rs, re - rs, v);
+    if (!g.elab) return p < re && __ldg(g.adj + p) == v;
+    for (; p < re && __ldg(g.adj + p) == v; ++p)
+        if (__ldg(g.elab + p) == lab) return true;
+    return false;
+}
+
+struct StepArgs {
+    GraphView g;
+    const DQuery *__restrict__ plans;
+    uint32_t depth;
+    // parents: SoA columns (qid, m_0 .. m_{depth-1}), column c at ptup + c*pstride
+    const uint32_t *__restrict__ ptup;
+    uint64_t pstride;
+    const uint32_t *__restrict__ pcstart;
+    const unsigned long long *__restrict__ pcoff;  // [np+1]
+    uint64_t np;
+    const uint32_t *__restrict__ tile_parent;       // [ntiles+1]
+    unsigned long long c0, cend;
+    uint32_t ntiles;
+    // children: SoA columns (qid, m_0 .. m_depth)
+    uint32_t *ctup;
+    uint64_t cstride, ccap;
+    uint32_t *ccstart;
+    unsigned long long *ccoff;                      // [ccap+1]
+    // look-back
+    TileStatus *status;
+    uint32_t epoch;
+    uint32_t *tile_ctr;
+    // results
+    unsigned long long *counts;                     // per query
+    StepResult *result;
+    // mapping capture at the final depth (optional)
+    uint32_t *rows_out;
+    uint64_t max_rows;
+    uint32_t *rows_ctr;
+};
+
+__global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_t np, unsigned long long c0,
+                            unsigned long long ncand, uint32_t ntiles, uint32_t *__restrict__ tile_parent,
+                            uint32_t *tile_ctr, StepResult *result) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        *tile_ctr = 0;
+        result->n_children = 0;
+        result->total_next = 0;
+        result->alg_bytes = 0;
+        result->err = 0;
+        result->rows = 0;
+    }
+    if (t > ntiles) return;
+    const unsigned long long c = c0 + (t < ntiles ? (unsigned long long)t * TILE : ncand - 1);
+    uint64_t lo = 0, hi = np;  // largest p with coff[p] <= c
+    while (hi - lo > 1) {
+        uint64_t mid = lo + ((hi - lo) >> 1);
+        if (coff[mid] <= c) lo = mid; else hi = mid;
+    }
+    tile_parent[t] = (uint32_t)lo;
+}
+
+template <typename V>
+__device__ __forceinline__ V warp_incl_scan(V x, uint32_t lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        V y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    return x;
+}
+template <typename V>
+__device__ __forceinline__ V warp_sum(V x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+template <bool ROOT>
+__global__ void __launch_bounds__(T) k_step(const StepArgs a) {
+    __shared__ unsigned long long s_coff[WIN];
+    __shared__ uint32_t s_wcnt[CPT][NWARP];
+    __shared__ unsigned long long s_wdeg[CPT][NWARP];
+    __shared__ unsigned long long s_wbytes[NWARP];
+    __shared__ uint32_t s_tile, s_q0;
+    __shared__ unsigned long long s_excl_cnt, s_excl_deg, s_agg_cnt, s_agg_deg, s_fcount;
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
+        s_fcount = 0;
+    }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const unsigned long long base = a.c0 + (unsigned long long)tile * TILE;
+    const uint32_t plo = a.tile_parent[tile], phi = a.tile_parent[tile + 1];
+    const uint32_t nwin = phi - plo + 2;  // coff[plo .. phi+1]
+    const bool win_smem = nwin <= (uint32_t)WIN;
+    if (win_smem)
+        for (uint32_t i = tid; i < nwin; i += T) s_coff[i] = a.pcoff[plo + i];
+    if (tid == 0) s_q0 = ROOT ? plo : a.ptup[plo];
+    __syncthreads();
+
+    const uint32_t d = a.depth;
+    uint32_t cpar[CPT], cv[CPT], cst[CPT], ccnt[CPT];
+    bool cemit[CPT];
+    unsigned long long my_bytes = 0;
+    uint32_t fq = 0xffffffffu;
+    unsigned long long fc = 0;
+
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+        cemit[j] = false;
+        cpar[j] = 0; cv[j] = 0; cst[j] = 0; ccnt[j] = 0;
+        const unsigned long long c = base + (unsigned long long)(j * T) + tid;
+        if (c >= a.cend) continue;
+        // parent = largest p in [plo, phi] with coff[p] <= c
+        uint32_t lo = 0, hi = nwin - 1;
+        if (win_smem) {
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (s_coff[mid] <= c) lo = mid; else hi = mid;
+            }
+        } else {
+            while (hi - lo > 1) {
+                uint32_t mid = lo + ((hi - lo) >> 1);
+                if (a.pcoff[plo + mid] <= c) lo = mid; else hi = mid;
+            }
+        }
+        const uint32_t p = plo + lo;
+        const unsigned long long pc = win_smem ? s_coff[lo] : a.pcoff[p];
+        const uint32_t local = (uint32_t)(c - pc);
+        const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
+        const DLevel *L = &a.plans[q].lv[d];
+        uint32_t v;
+        bool pass = true;
+        if (ROOT) {
+            v = __ldg(a.pcstart + p) + local;
+            my_bytes += 4;  // degree/label read of a data vertex
+        } else {
+            const uint32_t idx = __ldg(a.pcstart + p) + local;
+            v = __ldg(a.g.adj + idx);
+            const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
+            if (L->anchor_check) pass = has_edge(a.g, anchor, v, L->anchor_lab);
+            else if (a.g.elab) pass = __ldg(a.g.elab + idx) == L->anchor_lab;
+            // injectivity (HnGPU.cu:223-236)
+#pragma unroll
+            for (int i = 0; i < MAXQ; ++i)
+                if ((uint32_t)i < d && __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+            if (local == 0) {
+                // algorithmic bytes of this parent: its tuple and every backward
+                // neighbour's row (anchor + requirement rows), read once
+                unsigned long long b = 4ull * d;
+                b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
+                for (uint32_t r = 0; r < L->nreq; ++r) {
+                    const uint32_t pos = L->req_pos[r];
+                    if (pos == REQ_SELF) continue;
+                    const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                    b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
+                }
+                my_bytes += b;
+            }
+        }
+        // remaining requirements (HnGPU.cu:243-252)
+        for (uint32_t r = 0; r < L->nreq && pass; ++r) {
+            const uint32_t pos = L->req_pos[r];
+            const uint32_t u = pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+            pass = has_edge(a.g, u, v, L->req_lab[r]);
+        }
+        if (!pass) continue;
+        if (L->final_) {
+            if (a.rows_out) {
+                const uint32_t slot = atomicAdd(a.rows_ctr, 1u);
+                if (slot < a.max_rows) {
+                    const DQuery *Q = &a.plans[q];
+                    uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
+                    for (uint32_t i = 0; i < d; ++i)
+                        row[Q->col[i]] = __ldg(a.g.order + __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
+                    row[Q->col[d]] = __ldg(a.g.order + v);
+                }
+            }
+            if (fc && q != fq) {
+                atomicAdd(&a.counts[fq], fc);
+                fc = 0;
+            }
+            fq = q;
+            ++fc;
+            continue;
+        }
+        // the child's own candidate slice for depth+1
+        const uint32_t na = L->next_anchor;
+        const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+        const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
+        const uint32_t s = L->next_lo ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo) : rs;
+        const uint32_t e = L->next_hi < a.g.n ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi) : re;
+        if (e > s) {  // a child with no candidates cannot be extended: not written
+            cemit[j] = true;
+            cpar[j] = p;
+            cv[j] = v;
+            cst[j] = s;
+            ccnt[j] = e - s;
+        }
+    }
+
+    // ---- final-depth counts: one shared add per warp in the common case
+    {
+        const bool uniform = __all_sync(0xffffffffu, fc == 0 || fq == s_q0);
+        if (uniform) {
+            const unsigned long long sum = warp_sum(fc);
+            if (lane == 0 && sum) atomicAdd(&s_fcount, sum);
+        } else if (fc) {
+            atomicAdd(&a.counts[fq], fc);
+        }
+    }
+    // ---- rank the children in (j, thread) order
+    {
+        const unsigned long long wb = warp_sum(my_bytes);
+        if (lane == 0) s_wbytes[warp] = wb;
+    }
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, cemit[j]);
+        const unsigned long long dg = warp_incl_scan<unsigned long long>(cemit[j] ? ccnt[j] : 0ull, lane);
+        if (lane == 31) {
+            s_wcnt[j][warp] = __popc(bal);
+            s_wdeg[j][warp] = dg;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long cc = 0, dd = 0, bb = 0;
+        for (int j = 0; j < CPT; ++j)
+            for (int w = 0; w < NWARP; ++w) {
+                const uint32_t x = s_wcnt[j][w];
+                const unsigned long long y = s_wdeg[j][w];
+                s_wcnt[j][w] = (uint32_t)cc;
+                s_wdeg[j][w] = dd;
+                cc += x;
+                dd += y;
+            }
+        for (int w = 0; w < NWARP; ++w) bb += s_wbytes[w];
+        s_agg_cnt = cc;
+        s_agg_deg = dd;
+        if (bb) atomicAdd(&a.result->alg_bytes, bb);
+        if (s_fcount) atomicAdd(&a.counts[s_q0], s_fcount);
+    }
+    __syncthreads();
+    // ---- decoupled look-back (warp 0)
+    if (warp == 0) {
+        const uint32_t agg_cnt = (uint32_t)s_agg_cnt;
+        const unsigned long long agg_deg = s_agg_deg;
+        unsigned long long ex_cnt = 0, ex_deg = 0;
+        TileStatus *st = a.status;
+        if (tile == 0) {
+            if (lane == 0) {
+                st[0].inc_deg = agg_deg;
+                st_release(&st[0].word, status_word(a.epoch, FLAG_INC, agg_cnt));
+            }
+        } else {
+            if (lane == 0) {
+                st[tile].agg_deg = agg_deg;
+                st_release(&st[tile].word, status_word(a.epoch, FLAG_AGG, agg_cnt));
+            }
+            long long pred = (long long)tile - 1;
+            uint32_t spins = 0;
+            bool failed = false;
+            for (;;) {
+                const long long idx = pred - (long long)lane;
+                unsigned long long w = 0;
+                uint32_t flag = FLAG_INC;
+                for (;;) {
+                    if (idx >= 0) {
+                        w = ld_acquire(&st[idx].word);
+                        flag = (uint32_t)(w >> 34) == a.epoch ? (uint32_t)(w >> 32) & 3u : 0u;
+                    }
+                    if (__all_sync(0xffffffffu, flag != 0)) break;
+                    if (++spins > SPIN_LIMIT) { failed = true; break; }
+                    __nanosleep(64);
+                }
+                if (failed) break;
+                const uint32_t incm = __ballot_sync(0xffffffffu, flag == FLAG_INC);
+                const int first = incm ? __ffs(incm) - 1 : 32;
+                unsigned long long vc = 0, vd = 0;
+                if ((int)lane <= first && idx >= 0) {
+                    vc = (uint32_t)w;
+                    vd = flag == FLAG_INC ? __ldcg(&st[idx].inc_deg) : __ldcg(&st[idx].agg_deg);
+                }
+                ex_cnt += warp_sum(vc);
+                ex_deg += warp_sum(vd);
+                if (incm) break;
+                pred -= 32;
+            }
+            if (lane == 0) {
+                if (failed) atomicOr(&a.result->err, KERR_LOOKBACK);
+                st[tile].inc_deg = ex_deg + agg_deg;
+                st_release(&st[tile].word, status_word(a.epoch, FLAG_INC, (uint32_t)(ex_cnt + agg_cnt)));
+            }
+        }
+        if (lane == 0) {
+            s_excl_cnt = ex_cnt;
+            s_excl_deg = ex_deg;
+            if (tile == a.ntiles - 1) {
+                a.result->n_children = ex_cnt + agg_cnt;
+                a.result->total_next = ex_deg + agg_deg;
+                if (ex_cnt + agg_cnt <= a.ccap && a.ccoff) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- write children (SoA: consecutive children -> consecutive words per column)
+    const unsigned long long ex_cnt = s_excl_cnt, ex_deg = s_excl_deg;
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, cemit[j]);
+        const unsigned long long dg = warp_incl_scan<unsigned long long>(cemit[j] ? ccnt[j] : 0ull, lane);
+        if (!cemit[j]) continue;
+        const uint64_t slot = ex_cnt + s_wcnt[j][warp] + __popc(bal & ((1u << lane) - 1u));
+        if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
+        const uint32_t p = cpar[j];
+        const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
+        a.ctup[slot] = q;
+        for (uint32_t i = 0; i < d; ++i)
+            a.ctup[(uint64_t)(1 + i) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p);
+        a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = cv[j];
+        a.ccstart[slot] = cst[j];
+        a.ccoff[slot] = ex_deg + s_wdeg[j][warp] + dg - ccnt[j];
+    }
+}
+
+inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Device plan of one query against one data graph
+// ---------------------------------------------------------------------------
+gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim, DQuery &dq,
+                         uint32_t &root_lo, uint32_t &root_hi, bool &never) {
+    std::memset(&dq, 0, sizeof(dq));
+    never = false;
+    const uint32_t k = p.k;
+    if (k == 0 || k > (uint32_t)MAXQ) return GFSM_ERR_TOO_LARGE;
+    dq.k = k;
+    const bool use_deg = lim.degree_filter && g.symmetric && p.symmetric;
+    std::vector<uint32_t> lo(k), hi(k);
+    for (uint32_t d = 0; d < k; ++d) {
+        uint32_t glo = 0, ghi = g.n;
+        if (g.vl_grouped) {
+            auto it = std::lower_bound(g.group_value.begin(), g.group_value.end(), p.qlabel[d]);
+            if (it == g.group_value.end() || *it != p.qlabel[d]) { never = true; glo = ghi = 0; }
+            else {
+                size_t gi = (size_t)(it - g.group_value.begin());
+                glo = g.group_start[gi];
+                ghi = g.group_start[gi + 1];
+            }
+        }
+        // degree window: ids in a group are degree-descending, so
+        // "degree >= delta" is a prefix of the group.
+        uint32_t delta = use_deg ? p.qdeg[d] : 0;
+        if (d == 0) delta = std::max<uint32_t>(delta, 1);  // a root needs a CCSR row (HnGPU.cu:475-495)
+        uint32_t cut = ghi;
+        if (delta > 0) {
+            uint32_t a = glo, b = ghi;
+            while (a < b) {
+                uint32_t mid = a + (b - a) / 2;
+                if (g.degree(mid) >= delta) a = mid + 1; else b = mid;
+            }
+            cut = a;
+        }
+        lo[d] = glo;
+        hi[d] = cut;
+        if (lo[d] >= hi[d]) never = true;
+    }
+    for (uint32_t d = 0; d < k; ++d) {
+        DLevel &L = dq.lv[d];
+        L.lo = lo[d];
+        L.hi = hi[d];
+        L.final_ = d + 1 == k;
+        dq.col[d] = (uint8_t)p.qvid[d];
+        const uint32_t nreq = p.header[3 * d], roff = p.header[3 * d + 1], firstq = p.header[3 * d + 2];
+        uint32_t dist = 0, nr = 0;
+        bool anchor_done = false;
+        for (uint32_t r = 0; r < nreq; ++r) {
+            dist += p.reqs[roff + 2 * r];
+            const uint32_t rel = p.reqs[roff + 2 * r + 1];
+            if (!g.elab && g.m && rel != g.single_label) never = true;  // no such edge label in the data
+            if (d > 0 && !anchor_done && dist == firstq) {
+                anchor_done = true;
+                L.anchor = (uint8_t)(d - firstq);
+                L.anchor_lab = (uint8_t)rel;
+                L.anchor_check = g.multi ? 1 : 0;
+                continue;
+            }
+            if (nr >= (uint32_t)MAXQ) return GFSM_ERR_TOO_LARGE;
+            L.req_pos[nr] = dist == 0 ? REQ_SELF : (uint8_t)(d - dist);
+            L.req_lab[nr] = (uint8_t)rel;
+            ++nr;
+        }
+        if (d > 0 && !anchor_done) return GFSM_ERR_QUERY;
+        L.nreq = (uint8_t)nr;
+    }
+    for (uint32_t d = 0; d + 1 < k; ++d) {
+        DLevel &L = dq.lv[d];
+        const DLevel &N = dq.lv[d + 1];
+        L.next_anchor = N.anchor;
+        L.next_lo = N.lo;
+        L.next_hi = N.hi;
+    }
+    root_lo = lo[0];
+    root_hi = hi[0];
+    return GFSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+#define ECHECK(x)                                                               \
+    do {                                                                        \
+        cudaError_t e_ = (x);                                                   \
+        if (e_ != cudaSuccess) {                                                \
+            err = std::string(#x) + ": " + cudaGetErrorString(e_);              \
+            return e_ == cudaErrorMemoryAllocation ? GFSM_ERR_NOMEM : GFSM_ERR_CUDA; \
+        }                                                                       \
+    } while (0)
+
+Engine::~Engine() { release(); }
+
+void Engine::release() {
+    if (arena) cudaFree(arena);
+    if (small) cudaFree(small);
+    if (h_result) cudaFreeHost(h_result);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    arena = nullptr;
+    small = nullptr;
+    h_result = nullptr;
+    ev0 = ev1 = nullptr;
+    stream = nullptr;
+}
+
+gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std::string &err) {
+    device = dev;
+    ECHECK(cudaSetDevice(dev));
+    ECHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    ECHECK(cudaEventCreate(&ev0));
+    ECHECK(cudaEventCreate(&ev1));
+    ECHECK(cudaMallocHost(&h_result, sizeof(StepResult)));
+    max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
+    status_tiles = (uint32_t)div_up(max_scan, TILE);
+    // small region: tile status, tile directory, counters, result, plans
+    small_bytes = (uint64_t)status_tiles * sizeof(TileStatus) + ((uint64_t)status_tiles + 2) * 4 + 512;
+    ECHECK(cudaMalloc(&small, small_bytes));
+    ECHECK(cudaMemsetAsync(small, 0, small_bytes, stream));
+    char *p = static_cast<char *>(small);
+    status = reinterpret_cast<TileStatus *>(p);
+    p += (uint64_t)status_tiles * sizeof(TileStatus);
+    d_result = reinterpret_cast<StepResult *>(p);
+    p += 64;
+    tile_ctr = reinterpret_cast<uint32_t *>(p);
+    p += 64;
+    rows_ctr = reinterpret_cast<uint32_t *>(p);
+    p += 64;
+    tile_parent = reinterpret_cast<uint32_t *>(p);
+    arena_cap = arena_limit;
+    epoch = 0;
+    ECHECK(cudaStreamSynchronize(stream));
+    return GFSM_OK;
+}
+
+gfsm_status Engine::ensure_arena(uint64_t bytes, std::string &err) {
+    if (arena && arena_bytes >= bytes) return GFSM_OK;
+    if (arena) cudaFree(arena);
+    arena = nullptr;
+    arena_bytes = 0;
+    ECHECK(cudaMalloc(&arena, bytes));
+    arena_bytes = bytes;
+    return GFSM_OK;
+}
+
+gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
+                        uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
+                        uint64_t *n_rows, std::string &err) {
+    auto t_start = std::chrono::steady_clock::now();
+    const int nq = (int)plans.size();
+    gfsm_stats st{};
+    for (int i = 0; i < nq; ++i) counts_out[i] = 0;
+    if (n_rows) *n_rows = 0;
+    ECHECK(cudaSetDevice(device));
+
+    // device plans for the queries that can match at all
+    std::vector<DQuery> dq;
+    std::vector<int> active;
+    std::vector<uint32_t> rlo, rhi;
+    dq.reserve(nq);
+    uint32_t dmax = 0;
+    for (int i = 0; i < nq; ++i) {
+        DQuery q;
+        uint32_t lo = 0, hi = 0;
+        bool never = false;
+        gfsm_status rc = build_dquery(*plans[i], g, lim, q, lo, hi, never);
+        if (rc != GFSM_OK) return rc;
+        if (never) continue;
+        dq.push_back(q);
+        active.push_back(i);
+        rlo.push_back(lo);
+        rhi.push_back(hi);
+        dmax = std::max(dmax, q.k - 1);
+    }
+    const uint32_t na = (uint32_t)active.size();
+    if (na == 0) {
+        if (stats) {
+            st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+            *stats = st;
+        }
+        return GFSM_OK;
+    }
+    const uint64_t rows_bytes = rows_out ? max_rows * (uint64_t)dq[0].k * 4 : 0;
+
+    // arena layout: plans | counts | root coff | root cstart | mapping rows | depth buffers
+    const uint64_t plans_bytes = (uint64_t)na * sizeof(DQuery);
+    const uint64_t head = ((plans_bytes + 255) & ~255ull) + (((uint64_t)na * 8 + 255) & ~255ull) +
+                          ((((uint64_t)na + 1) * 8 + 255) & ~255ull) + (((uint64_t)na * 4 + 255) & ~255ull) +
+                          ((rows_bytes + 255) & ~255ull);
+    uint64_t budget = arena_cap;
+    if (budget <= head + (1ull << 20) * dmax) return GFSM_ERR_NOMEM;
+    gfsm_status rc = ensure_arena(budget, err);
+    if (rc != GFSM_OK) return rc;
+    char *p = static_cast<char *>(arena);
+    DQuery *d_plans = reinterpret_cast<DQuery *>(p);
+    p += (plans_bytes + 255) & ~255ull;
+    unsigned long long *d_counts = reinterpret_cast<unsigned long long *>(p);
+    p += ((uint64_t)na * 8 + 255) & ~255ull;
+    unsigned long long *d_rcoff = reinterpret_cast<unsigned long long *>(p);
+    p += (((uint64_t)na + 1) * 8 + 255) & ~255ull;
+    uint32_t *d_rcstart = reinterpret_cast<uint32_t *>(p);
+    p += ((uint64_t)na * 4 + 255) & ~255ull;
+    uint32_t *d_rows = rows_out ? reinterpret_cast<uint32_t *>(p) : nullptr;
+    p += (rows_bytes + 255) & ~255ull;
+
+    std::vector<unsigned long long> rcoff(na + 1, 0);
+    for (uint32_t i = 0; i < na; ++i) rcoff[i + 1] = rcoff[i] + (rhi[i] - rlo[i]);
+    ECHECK(cudaMemcpyAsync(d_plans, dq.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemsetAsync(d_counts, 0, (uint64_t)na * 8, stream));
+    ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)na + 1) * 8, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_rcstart, rlo.data(), (uint64_t)na * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
+
+    // depth buffers 0 .. dmax-1 (depth dmax is count-only)
+    const uint64_t rest = budget - (uint64_t)(p - static_cast<char *>(arena));
+    struct Buf {
+        uint32_t *tup;
+        uint64_t cap;
+        uint32_t *cstart;
+        unsigned long long *coff;
+    };
+    std::vector<Buf> buf(dmax);
+    {
+        const uint64_t share = dmax ? rest / dmax : 0;
+        for (uint32_t d = 0; d < dmax; ++d) {
+            const uint64_t per = 4ull * (d + 2) + 4 + 8;
+            uint64_t cap = share > 1024 ? (share - 1024) / per : 0;
+            cap = std::min<uint64_t>(cap, lim.max_soln_size);
+            cap = std::min<uint64_t>(cap, 0xffffffffull);
+            if (cap < TILE) return GFSM_ERR_NOMEM;
+            Buf &b = buf[d];
+            b.cap = cap;
+            char *q = p + share * d;
+            b.coff = reinterpret_cast<unsigned long long *>(q);
+            q += ((cap + 1) * 8 + 255) & ~255ull;
+            b.tup = reinterpret_cast<uint32_t *>(q);
+            q += (cap * 4 * (d + 2) + 255) & ~255ull;
+            b.cstart = reinterpret_cast<uint32_t *>(q);
+        }
+        st.peak_frontier_bytes = budget;
+    }
+
+    GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
+    std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0);
+    std::vector<double> ratio(dmax + 1, 1.0);
+    total[0] = rcoff[na];
+    np[0] = na;
+    uint32_t d = 0;
+    float kms = 0.f;
+    for (;;) {
+        if (pos[d] >= total[d]) {
+            if (d == 0) break;
+            --d;
+            continue;
+        }
+        const bool emits = d < dmax;
+        unsigned long long chunk = std::min<unsigned long long>(total[d] - pos[d], (unsigned long long)max_scan);
+        if (emits) {
+            const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
+            chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
+        }
+        const uint32_t ntiles = (uint32_t)div_up(chunk, TILE);
+        if (++epoch >= (1u << 30)) {
+            ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));
+            epoch = 1;
+        }
+        StepArgs a{};
+        a.g = gv;
+        a.plans = d_plans;
+        a.depth = d;
+        if (d == 0) {
+            a.ptup = nullptr;
+            a.pstride = 0;
+            a.pcstart = d_rcstart;
+            a.pcoff = d_rcoff;
+        } else {
+            a.ptup = buf[d - 1].tup;
+            a.pstride = buf[d - 1].cap;
+            a.pcstart = buf[d - 1].cstart;
+            a.pcoff = buf[d - 1].coff;
+        }
+        a.np = np[d];
+        a.tile_parent = tile_parent;
+        a.c0 = pos[d];
+        a.cend = pos[d] + chunk;
+        a.ntiles = ntiles;
+        if (emits) {
+            a.ctup = buf[d].tup;
+            a.cstride = buf[d].cap;
+            a.ccap = buf[d].cap;
+            a.ccstart = buf[d].cstart;
+            a.ccoff = buf[d].coff;
+        }
+        a.status = status;
+        a.epoch = epoch;
+        a.tile_ctr = tile_ctr;
+        a.counts = d_counts;
+        a.result = d_result;
+        a.rows_out = d_rows;
+        a.max_rows = max_rows;
+        a.rows_ctr = rows_ctr;
+        k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, stream>>>(
+            a.pcoff, a.np, a.c0, chunk, ntiles, tile_parent, tile_ctr, d_result);
+        ECHECK(cudaEventRecord(ev0, stream));
+        if (d == 0) k_step<true><<<ntiles, T, 0, stream>>>(a);
+        else k_step<false><<<ntiles, T, 0, stream>>>(a);
+        ECHECK(cudaGetLastError());
+        ECHECK(cudaEventRecord(ev1, stream));
+        ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
+        ECHECK(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        kms += ms;
+        st.steps++;
+        const StepResult r = *h_result;
+        if (r.err) {
+            err = "device step error bits " + std::to_string(r.err);
+            return (r.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
+        }
+        if (emits && r.n_children > buf[d].cap) {
+            // more survivors than the level buffer holds: redo a smaller chunk
+            st.retries++;
+            ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
+            continue;
+        }
+        st.candidates += chunk;
+        st.expansions += r.n_children;
+        st.alg_bytes += r.alg_bytes + (emits ? r.n_children * 4ull * (d + 1) : 0ull);
+        pos[d] += chunk;
+        if (emits) {
+            const double obs = (double)r.n_children / (double)chunk;
+            ratio[d] = std::max(2.0 * obs, ratio[d] * 0.5);
+            if (r.n_children > 0 && r.total_next > 0) {
+                np[d + 1] = r.n_children;
+                total[d + 1] = r.total_next;
+                pos[d + 1] = 0;
+                ++d;
+            }
+        }
+    }
+    std::vector<unsigned long long> cnt(na);
+    ECHECK(cudaMemcpyAsync(cnt.data(), d_counts, (uint64_t)na * 8, cudaMemcpyDeviceToHost, stream));
+    if (rows_out) ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
+    ECHECK(cudaStreamSynchronize(stream));
+    for (uint32_t i = 0; i < na; ++i) counts_out[active[i]] = cnt[i];
+    if (rows_out) {
+        uint64_t total_rows = 0;
+        for (uint32_t i = 0; i < na; ++i) total_rows += cnt[i];
+        const uint64_t nr = std::min<uint64_t>(total_rows, max_rows);
+        if (nr) ECHECK(cudaMemcpy(rows_out, d_rows, nr * dq[0].k * 4, cudaMemcpyDeviceToHost));
+        if (n_rows) *n_rows = nr;
+    }
+    for (uint32_t i = 0; i < na; ++i) st.count += cnt[i];
+    st.kernel_ms = kms;
+    st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    if (stats) *stats = st;
+    return GFSM_OK;
+}
+
+}  // namespace gfsm

@@ -1,0 +1,45 @@
+// engine.h -- one matching engine = one CUDA stream + one frontier arena.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "gfsm_internal.h"
+
+namespace gfsm {
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void *arena = nullptr;         // frontier buffers + per-call plans/counts
+    uint64_t arena_bytes = 0;
+    uint64_t arena_cap = 0;        // bytes the arena may use (MEMLIMIT share)
+    void *small = nullptr;         // tile status, tile directory, counters
+    uint64_t small_bytes = 0;
+    TileStatus *status = nullptr;
+    uint32_t status_tiles = 0;
+    StepResult *d_result = nullptr;
+    StepResult *h_result = nullptr;  // pinned
+    uint32_t *tile_ctr = nullptr;
+    uint32_t *rows_ctr = nullptr;
+    uint32_t *tile_parent = nullptr;
+    uint64_t max_scan = 0;
+    uint32_t epoch = 0;
+
+    Engine() = default;
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+    ~Engine();
+    void release();
+    gfsm_status init(int dev, uint64_t arena_limit, uint64_t scan_limit, std::string &err);
+    gfsm_status ensure_arena(uint64_t bytes, std::string &err);
+    // Counts every plan against g; counts_out[i] for plans[i].  With rows_out
+    // (single plan only) also writes up to max_rows full mappings.
+    gfsm_status run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
+                    uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
+                    uint64_t *n_rows, std::string &err);
+};
+
+}  // namespace gfsm

@@ -1,0 +1,154 @@
+// gfsm_internal.h -- host/device structures shared inside libgfsm.
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gfsm.h"
+
+namespace gfsm {
+
+constexpr int MAXQ = 16;              // query vertices supported by the device plan
+constexpr uint8_t REQ_SELF = 0xFF;    // requirement on the candidate's own row (query self-loop)
+
+// Environment.h:6-11 defaults.
+constexpr uint32_t kCCSRRelSize = 8;
+constexpr uint64_t kMaxSolnSize = 500'000'000ull;
+constexpr uint64_t kMaxScanSize = 500'000'000ull;
+constexpr uint64_t kMemLimit = 22'000'000'000ull;
+constexpr uint64_t kUpperMemLimit = 44'000'000'000ull;
+
+// ---------------------------------------------------------------------------
+// Host-side graph: the parsed edge lines, labels masked to CCSRRelSize bits.
+// ---------------------------------------------------------------------------
+struct HostGraph {
+    uint32_t n = 0;
+    std::vector<uint32_t> src, dst;   // directed entries, input order
+    std::vector<uint8_t> lab;         // edge label & ((1<<CCSRRelSize)-1)
+    std::vector<uint32_t> vlabel;     // per vertex id (v lines), 0 if absent
+};
+
+// Device CCSR.  Internal vertex ids are the reference's CCSR row order
+// (degree descending, then id ascending; HnHelper.cuh:26-31, 413), grouped by
+// vertex label first when vertex labels are matched.  Rows list neighbour
+// internal ids ascending (HnHelper.cuh:470-478).
+struct DeviceGraph {
+    int device = 0;
+    uint32_t n = 0, rows = 0, max_degree = 0;
+    uint64_t m = 0;
+    uint32_t *rowptr = nullptr;       // [n+1]
+    uint32_t *adj = nullptr;          // [m]
+    uint8_t *elab = nullptr;          // [m], null when every entry has the same label
+    uint32_t single_label = 0;        // the label when elab == null
+    uint32_t *order = nullptr;        // [n] internal id -> original id
+    bool symmetric = false, multi = false;
+    int n_edge_labels = 0;
+    bool vl_grouped = false;
+    // host copies used by the planner (degree windows) and for output
+    std::vector<uint32_t> h_rowptr;   // [n+1]
+    std::vector<uint32_t> h_order;    // [n]
+    std::vector<uint32_t> group_value;// sorted distinct vertex label values (grouped mode)
+    std::vector<uint32_t> group_start;// [groups+1]
+    uint64_t bytes = 0;
+    uint32_t degree(uint32_t v) const { return h_rowptr[v + 1] - h_rowptr[v]; }
+};
+
+// ---------------------------------------------------------------------------
+// Query plan (host).  The reference tables plus what the device plan needs.
+// ---------------------------------------------------------------------------
+struct Plan {
+    uint32_t k = 0, max_valency = 0;
+    uint32_t rel_bits = 8;           // CCSRRelSize the query was parsed with
+    std::vector<uint32_t> order;     // depth -> query CCSR row index
+    std::vector<uint32_t> header;    // [3k]
+    std::vector<uint32_t> reqs;      // [2*maxv*k] (distance delta, label value)
+    std::vector<uint32_t> qvid;      // depth -> query vertex id
+    std::vector<uint32_t> qlabel;    // depth -> query vertex label value
+    std::vector<uint32_t> qdeg;      // depth -> distinct non-self neighbours
+    bool symmetric = false;          // query structure is symmetric
+};
+
+// Per-depth device plan of one query against one data graph.
+struct alignas(16) DLevel {
+    uint32_t lo, hi;           // candidate id window of this depth
+    uint32_t next_lo, next_hi; // window of depth+1
+    uint8_t anchor;            // tuple position of the anchor (depth index)
+    uint8_t next_anchor;       // anchor position for depth+1
+    uint8_t nreq;              // extra requirement checks
+    uint8_t anchor_lab;        // label of the anchor requirement
+    uint8_t final_;            // depth == k-1
+    uint8_t anchor_check;      // anchor requirement needs a row search (multi-edge data)
+    uint8_t pad0, pad1;
+    uint8_t req_pos[MAXQ];     // tuple position, or REQ_SELF
+    uint8_t req_lab[MAXQ];
+};
+static_assert(sizeof(DLevel) == 64, "DLevel layout");
+
+struct alignas(16) DQuery {
+    DLevel lv[MAXQ];
+    uint8_t col[MAXQ];         // depth -> output column (query vertex id)
+    uint32_t k;
+    uint32_t pad[3];
+};
+
+struct StepResult {
+    unsigned long long n_children;
+    unsigned long long total_next;
+    unsigned long long alg_bytes;
+    unsigned int err;          // KERR_* bits
+    unsigned int rows;         // mapping rows claimed (mapping mode)
+};
+
+struct TileStatus {
+    unsigned long long word;   // epoch:30 | flag:2 | count:32
+    unsigned long long agg_deg;
+    unsigned long long inc_deg;
+    unsigned long long pad;
+};
+
+// Error bits raised by kernels (read by the host after each step).
+enum : uint32_t {
+    KERR_LOOKBACK = 1u,        // bounded look-back wait ran out
+    KERR_WINDOW = 2u,          // parent window larger than expected
+    KERR_BOUNDS = 4u,          // a vertex id out of range
+};
+
+}  // namespace gfsm
+
+// ---------------------------------------------------------------------------
+// Opaque C handles
+// ---------------------------------------------------------------------------
+struct gfsm_ctx {
+    gfsm_limits lim{};
+    int device = 0;
+    std::string last_error;
+    std::mutex mu;
+    void *engine = nullptr;   // default gfsm::Engine (stream + frontier arena)
+};
+
+struct gfsm_graph {
+    gfsm_ctx *ctx = nullptr;
+    gfsm::HostGraph h;
+    gfsm::DeviceGraph *dev = nullptr;
+    uint32_t rel_bits = 8;
+    bool vl_mode = false;
+};
+
+struct gfsm_plan {
+    gfsm::Plan p;
+};
+
+namespace gfsm {
+// host_graph.cpp
+gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGraph &g);
+gfsm_status read_file(const char *path, std::string &out);
+gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p);
+// builder.cu
+gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, DeviceGraph &out,
+                               std::string &err);
+void free_device_graph(DeviceGraph &g);
+// engine.cu
+gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim,
+                         DQuery &dq, uint32_t &root_lo, uint32_t &root_hi, bool &never);
+}  // namespace gfsm

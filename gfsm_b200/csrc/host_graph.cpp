@@ -1,0 +1,301 @@
+// host_graph.cpp -- text ingest and query planning (host side of libgfsm).
+//
+// parse_text restates the reference parser's semantics (HnHelper.cuh:191-266
+// parseValues, :283-381 fileParse) but runs multi-threaded over line-aligned
+// chunks: the reference reads the file byte by byte on one thread.
+// plan_query restates the reference's matching order and requirement table
+// (HnGPU.cu:749-816 preProcessQuery, ccsr.cpp:98-219).
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+#include "gfsm_internal.h"
+
+namespace gfsm {
+
+namespace {
+
+enum LineKind : uint8_t { L_V, L_E, L_END, L_BAD };
+
+// Tokenises one line the way parseValues does (HnHelper.cuh:233-263): digit
+// runs accumulate into the current value slot with uint32 wrap-around, every
+// other byte moves to the next slot, '\n' ends the line.
+inline const char *scan_values(const char *s, const char *end, uint32_t *v, int nv) {
+    uint32_t cur = 0;
+    for (; s < end; ++s) {
+        char ch = *s;
+        if (ch >= '0' && ch <= '9') {
+            if ((int)cur < nv) v[cur] = v[cur] * 10u + (uint32_t)(ch - '0');
+        } else {
+            ++cur;
+            if (ch == '\n') return s + 1;
+        }
+    }
+    return s;
+}
+
+struct ChunkOut {
+    std::vector<uint32_t> es, ed, el;      // edge lines
+    std::vector<uint32_t> vid, vlab;       // vertex lines
+    uint64_t first_stop = UINT64_MAX;      // byte offset of the first 't' or bad line
+    LineKind stop_kind = L_END;
+    uint64_t first_e = UINT64_MAX;         // byte offset of the first 'e' line
+    uint64_t last_v = 0;                   // byte offset of the last 'v' line (+1), 0 if none
+    // per-line order for validation: offsets of the first 'v' after an 'e'
+    uint64_t first_v_after_e = UINT64_MAX;
+};
+
+void scan_chunk(const char *buf, uint64_t b, uint64_t e, uint64_t len, ChunkOut &o) {
+    const char *end = buf + len;
+    uint64_t pos = b;
+    while (pos < e) {
+        const char *line = buf + pos;
+        char ch = *line;
+        const char *nl = static_cast<const char *>(memchr(line, '\n', len - pos));
+        const char *lend = nl ? nl + 1 : end;
+        if (ch == 't') {
+            bool ok = (uint64_t)(end - line) >= 6 && !strncmp(line, "t # -1", 6);
+            o.first_stop = pos;
+            o.stop_kind = ok ? L_END : L_BAD;
+            return;
+        }
+        if (ch == 'v' || ch == 'e') {
+            uint32_t v[3] = {0, 0, 0};
+            const char *vs = line + 2 < lend ? line + 2 : lend;
+            scan_values(vs, lend, v, 3);
+            if (ch == 'v') {
+                o.vid.push_back(v[0]);
+                o.vlab.push_back(v[1]);
+                o.last_v = pos + 1;
+                if (o.first_e != UINT64_MAX && o.first_v_after_e == UINT64_MAX) o.first_v_after_e = pos;
+            } else {
+                if (o.first_e == UINT64_MAX) o.first_e = pos;
+                o.es.push_back(v[0]);
+                o.ed.push_back(v[1]);
+                o.el.push_back(v[2]);
+            }
+        } else {
+            o.first_stop = pos;
+            o.stop_kind = L_BAD;
+            return;
+        }
+        pos = (uint64_t)(lend - buf);
+    }
+}
+
+}  // namespace
+
+gfsm_status read_file(const char *path, std::string &out) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return GFSM_ERR_MISSING_FILE;  // HnHelper.cuh:289-294
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    rewind(f);
+    out.resize(sz > 0 ? (size_t)sz : 0);
+    size_t got = sz > 0 ? fread(&out[0], 1, (size_t)sz, f) : 0;
+    fclose(f);
+    out.resize(got);
+    return GFSM_OK;
+}
+
+gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGraph &g) {
+    g = HostGraph();
+    if (len < 6 || strncmp(buf, "t # 0\n", 6)) return GFSM_ERR_INVALID_DATA;  // :312-314
+    // Header line (parseValues in header mode, :206-210): values 0 and 1 are
+    // the vertex and edge-line counts.
+    uint64_t pos = 6;
+    uint32_t hv[4] = {0, 0, 0, 0};
+    if (pos < len && buf[pos] == 't') {
+        if (len - pos < 6 || strncmp(buf + pos, "t # -1", 6)) return GFSM_ERR_INVALID_DATA;
+        return GFSM_OK;  // empty graph
+    }
+    const char *after = scan_values(buf + pos, buf + len, hv, 4);
+    const uint32_t n = hv[0], ecount = hv[1];
+    pos = (uint64_t)(after - buf);
+
+    // Line-aligned chunks, scanned in parallel.
+    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    uint64_t body = len - pos;
+    unsigned nt = (unsigned)std::min<uint64_t>(hw, std::max<uint64_t>(1, body / (1u << 20)));
+    std::vector<uint64_t> cut(nt + 1);
+    cut[0] = pos;
+    cut[nt] = len;
+    for (unsigned t = 1; t < nt; ++t) {
+        uint64_t c = pos + body * t / nt;
+        const char *nl = static_cast<const char *>(memchr(buf + c, '\n', len - c));
+        c = nl ? (uint64_t)(nl - buf) + 1 : len;
+        cut[t] = std::max(c, cut[t - 1]);
+    }
+    std::vector<ChunkOut> outs(nt);
+    {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] { scan_chunk(buf, cut[t], cut[t + 1], len, outs[t]); });
+        for (auto &x : th) x.join();
+    }
+    // Sequential semantics: the parse stops at the first 't' line or bad
+    // line; a bad line (or a 'v' line inside the edge section, or a 't' line
+    // other than "t # -1") before that point is ERR_INVALID_DATA.
+    unsigned stop_chunk = nt;
+    for (unsigned t = 0; t < nt; ++t)
+        if (outs[t].first_stop != UINT64_MAX) { stop_chunk = t; break; }
+    if (stop_chunk < nt && outs[stop_chunk].stop_kind == L_BAD) return GFSM_ERR_INVALID_DATA;
+    unsigned last = stop_chunk < nt ? stop_chunk : nt - 1;
+    bool seen_e = false;
+    uint64_t nv = 0, ne = 0;
+    for (unsigned t = 0; t <= last; ++t) {
+        const ChunkOut &o = outs[t];
+        if (o.first_v_after_e != UINT64_MAX) return GFSM_ERR_INVALID_DATA;
+        if (seen_e && !o.vid.empty()) return GFSM_ERR_INVALID_DATA;
+        if (!o.es.empty()) seen_e = true;
+        nv += o.vid.size();
+        ne += o.es.size();
+    }
+    // vertexSeen also counts the 'e' line that ends the vertex section (:344).
+    uint64_t vseen = nv + (ne > 0 ? 1 : 0);
+    if (vseen < n) return GFSM_ERR_MISSING_DATA;   // :347-349
+    if (ne < ecount) return GFSM_ERR_MISSING_DATA; // :379-381
+
+    g.n = n;
+    g.vlabel.assign(n, 0);
+    g.src.resize(ne);
+    g.dst.resize(ne);
+    g.lab.resize(ne);
+    const uint32_t vert_bits = 32u - rel_bits;
+    uint64_t w = 0;
+    for (unsigned t = 0; t <= last; ++t) {
+        const ChunkOut &o = outs[t];
+        for (size_t i = 0; i < o.vid.size(); ++i)
+            if (o.vid[i] < n) g.vlabel[o.vid[i]] = o.vlab[i];
+        for (size_t i = 0; i < o.es.size(); ++i, ++w) {
+            if (o.es[i] >= n || o.ed[i] >= n) return GFSM_ERR_INVALID_DATA;  // reference: out of bounds
+            g.src[w] = o.es[i];
+            g.dst[w] = o.ed[i];
+            // (label << CCSRVertSize) keeps the low CCSRRelSize bits (:376)
+            g.lab[w] = (uint8_t)(((uint32_t)(o.el[i] << vert_bits)) >> vert_bits);
+        }
+    }
+    return GFSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Planner
+// ---------------------------------------------------------------------------
+gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p) {
+    p = Plan();
+    p.rel_bits = rel_bits;
+    const uint32_t k = q.n;
+    if (k == 0) return GFSM_ERR_QUERY;
+    if (k > (uint32_t)MAXQ) return GFSM_ERR_TOO_LARGE;
+    std::vector<uint32_t> deg(k, 0);
+    for (uint32_t s : q.src) deg[s]++;
+    for (uint32_t v = 0; v < k; ++v)
+        if (!deg[v]) return GFSM_ERR_QUERY;  // no row: the reference walks past its CCSR
+    // Query CCSR rows: degree descending, id ascending (HnHelper.cuh:26-31).
+    std::vector<uint32_t> rowvid(k), rowidx(k);
+    for (uint32_t v = 0; v < k; ++v) rowvid[v] = v;
+    std::stable_sort(rowvid.begin(), rowvid.end(),
+                     [&](uint32_t a, uint32_t b) { return deg[a] > deg[b]; });
+    for (uint32_t i = 0; i < k; ++i) rowidx[rowvid[i]] = i;
+    // rows[i] = (target row, label) sorted by target (HnHelper.cuh:470-478)
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> rows(k);
+    for (size_t e = 0; e < q.src.size(); ++e)
+        rows[rowidx[q.src[e]]].push_back({rowidx[q.dst[e]], q.lab[e]});
+    uint32_t maxv = 0;
+    for (auto &r : rows) {
+        std::stable_sort(r.begin(), r.end(),
+                         [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
+                             return a.first < b.first;
+                         });
+        maxv = std::max<uint32_t>(maxv, (uint32_t)r.size());
+    }
+    p.k = k;
+    p.max_valency = maxv;
+    p.order.assign(k, 0);
+    p.header.assign(3 * (size_t)k, 0);
+    p.reqs.assign(2 * (size_t)maxv * k, 0);
+    std::vector<int32_t> mapping(k, -1);
+    mapping[0] = 0;  // HnGPU.cu:759-769: the first row has the maximal degree
+    for (uint32_t depth = 0; depth < k; ++depth) {  // HnGPU.cu:771-773
+        // ccsr.cpp:114-123
+        uint32_t rel_depth = 0;
+        bool found = false;
+        for (uint32_t i = 0; i < k; ++i) {
+            if (mapping[i] == 0 && !found) {
+                mapping[i] = 1;
+                rel_depth = i;
+                found = true;
+            } else if (mapping[i] > 0) {
+                mapping[i]++;
+            }
+        }
+        if (!found) return GFSM_ERR_QUERY;  // ccsr.cpp:126-128
+        p.order[depth] = rel_depth;
+        // ccsr.cpp:142-167
+        std::vector<std::pair<uint32_t, uint32_t>> rr;
+        for (auto &ent : rows[rel_depth]) {
+            uint32_t t = ent.first;
+            if (mapping[t] < 0) mapping[t] = 0;
+            if (mapping[t] > 0) {
+                uint32_t rel = ent.second;
+                for (auto &back : rows[t])
+                    if (back.first == rel_depth) { rel = back.second; break; }
+                rr.push_back({(uint32_t)(mapping[t] - 1), rel});
+            }
+        }
+        // ccsr.cpp:169-196
+        uint32_t firstq = 0, off = depth * maxv * 2;
+        if (!rr.empty()) {
+            std::stable_sort(rr.begin(), rr.end(),
+                             [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
+                                 return a.first < b.first;
+                             });
+            p.reqs[off] = rr[0].first;
+            p.reqs[off + 1] = rr[0].second;
+            for (size_t i = 1; i < rr.size(); ++i) {
+                p.reqs[off + 2 * i] = rr[i].first - rr[i - 1].first;
+                p.reqs[off + 2 * i + 1] = rr[i].second;
+            }
+            firstq = p.reqs[off];
+            for (size_t i = 0; i < rr.size(); ++i) {
+                firstq = p.reqs[off + 2 * i];
+                if (firstq) break;
+            }
+        }
+        if ((firstq > depth && depth) || (depth && !firstq)) return GFSM_ERR_QUERY;
+        p.header[depth * 3 + 0] = (uint32_t)rr.size();
+        p.header[depth * 3 + 1] = off;
+        p.header[depth * 3 + 2] = firstq;
+    }
+    for (size_t i = 0; i < (size_t)maxv * k; ++i)  // HnGPU.cu:807-813
+        if (p.reqs[i * 2] > k) return GFSM_ERR_QUERY;
+
+    // What the device plan needs beyond the reference tables.
+    p.qvid.resize(k);
+    p.qlabel.resize(k);
+    p.qdeg.resize(k);
+    for (uint32_t d = 0; d < k; ++d) {
+        uint32_t v = rowvid[p.order[d]];
+        p.qvid[d] = v;
+        p.qlabel[d] = v < q.vlabel.size() ? q.vlabel[v] : 0;
+        std::vector<uint32_t> nb;
+        for (auto &ent : rows[p.order[d]])
+            if (ent.first != p.order[d]) nb.push_back(ent.first);
+        std::sort(nb.begin(), nb.end());
+        p.qdeg[d] = (uint32_t)(std::unique(nb.begin(), nb.end()) - nb.begin());
+    }
+    bool sym = true;
+    for (uint32_t u = 0; u < k && sym; ++u)
+        for (auto &ent : rows[u]) {
+            bool back = false;
+            for (auto &b : rows[ent.first])
+                if (b.first == u) { back = true; break; }
+            if (!back) { sym = false; break; }
+        }
+    p.symmetric = sym;
+    return GFSM_OK;
+}
+
+}  // namespace gfsm

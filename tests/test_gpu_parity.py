@@ -1,0 +1,240 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the oracle.
+
+Bit-exact integer counts (and, for small cases, identical sorted mapping
+sets) on: the golden fixtures; seeded random graphs and random-walk queries
+(trees and cyclic, edge labels, vertex labels); edge cases (no match, absent
+labels, query larger than data, duplicate entries, self-loops); forced
+chunking with tiny MEMLIMIT / MAXSCANSIZE / MAXSOLNSIZE; batched == one at a
+time; and size-independent closed forms at the full R-MAT 2^20 size."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import gfsm_b200
+from gfsm_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+COUNTS = json.load(open(os.path.join(GOLD, "counts.json")))
+
+
+def _g(key):
+    return os.path.join(GOLD, key + ".g")
+
+
+@pytest.mark.parametrize("key", sorted(COUNTS))
+def test_golden_counts(gpu_ctx, gpu_ctx_vl, key):
+    qn, dn = key.split("|")
+    for ctx, field in ((gpu_ctx, "count"), (gpu_ctx_vl, "count_vlabels")):
+        q = ctx.file_parse(_g("queries/" + qn))
+        d = ctx.file_parse(_g("data/" + dn))
+        assert ctx.solve(q, d) == COUNTS[key][field]
+
+
+def _labelled_query(g, lab, qg, visited):
+    if lab is None:
+        return None
+    key = {(int(a), int(b)): int(l) for a, b, l in zip(g.src, g.dst, lab)}
+    return np.array([key[(min(visited[a], visited[b]), max(visited[a], visited[b]))]
+                     for a, b in zip(qg.src, qg.dst)], np.uint32)
+
+
+def _both_dirs(ug, lab=None):
+    s, d = ug.directed()
+    l = None if lab is None else np.concatenate([lab, lab])
+    return s, d, l
+
+
+GENS = [
+    ("er", lambda s: synth.er(400, 6.0, seed=s)),
+    ("ba", lambda s: synth.ba(500, 3, seed=s)),
+    ("rmat", lambda s: synth.rmat(9, 2500, seed=s)),
+    ("grid", lambda s: synth.grid(20, 0.05, 0.03, seed=s)),
+]
+
+
+@pytest.mark.parametrize("gen", range(len(GENS)))
+@pytest.mark.parametrize("labelled", [False, True])
+def test_random_walk_queries(gpu_ctx, gpu_ctx_vl, tmp_path, gen, labelled):
+    name, fn = GENS[gen]
+    g = fn(gen + 1)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=gen + 40)
+    lab = ((np.arange(g.m, dtype=np.uint64) * 2654435761 + gen) % 3 + 1).astype(np.uint32) if labelled else None
+    dpath = tmp_path / "d.g"
+    g.write_text(str(dpath), lab)
+    od = O.Graph(path=str(dpath))
+    ds, dd, dl = _both_dirs(g, lab)
+    dev = {c: c.graph_from_edges(g.n, ds, dd, dl, g.vlabel) for c in (gpu_ctx, gpu_ctx_vl)}
+    text_graph = gpu_ctx.file_parse(str(dpath))
+    for i, k in enumerate((3, 4, 5, 6, 7)):
+        for tree in (False, True):
+            qg, visited = synth.rw_query(g, k, tree=tree, seed=1000 * gen + 10 * i + tree)
+            ql = _labelled_query(g, lab, qg, visited)
+            qpath = tmp_path / "q.g"
+            qg.write_text(str(qpath), ql)
+            oq = O.Graph(path=str(qpath))
+            op = O.Plan(oq)
+            want = O.ffs_count(oq, op, od, threads=8)
+            want_vl = O.ffs_count(oq, op, od, vlabel_mode=True, threads=8)
+            for ctx, expect in ((gpu_ctx, want), (gpu_ctx_vl, want_vl)):
+                plan = ctx.pre_process_query(ctx.file_parse(str(qpath)))
+                got, st = ctx.match_count(plan, dev[ctx])
+                assert got == expect, (name, k, tree, ctx is gpu_ctx_vl, got, expect)
+            # the text-parsed data graph gives the same count
+            plan = gpu_ctx.pre_process_query(gpu_ctx.file_parse(str(qpath)))
+            assert gpu_ctx.match_count(plan, text_graph)[0] == want
+
+
+def test_mappings_match_backtracking(gpu_ctx, tmp_path):
+    g = synth.er(120, 5.0, seed=9)
+    ds, dd, _ = _both_dirs(g)
+    data = gpu_ctx.graph_from_edges(g.n, ds, dd)
+    for qn in ("_3_triangle", "_4_square", "_5_plus", "_5_road5"):
+        oq = O.Graph(path=_g("queries/" + qn))
+        qs, qd, ql = oq.edges()
+        k = oq.arrays()["count"]
+        c2, r2 = O.bt_count(k, qs, qd, ql, None, g.n, ds, dd, None, None, threads=8, max_rows=2_000_000)
+        plan = gpu_ctx.pre_process_query(gpu_ctx.file_parse(_g("queries/" + qn)))
+        rows, c1 = gpu_ctx.match_mappings(plan, data, max_rows=2_000_000)
+        assert c1 == c2 == len(rows) == len(r2)
+        s1 = rows[np.lexsort(rows.T[::-1])]
+        s2 = r2[np.lexsort(r2.T[::-1])]
+        assert np.array_equal(s1, s2)
+
+
+def test_edge_cases(gpu_ctx, gpu_ctx_vl, tmp_path):
+    tri = gpu_ctx.file_parse(_g("queries/_3_triangle"))
+    # a tree has no triangle
+    path = synth.UGraph(6, np.arange(5, dtype=np.uint32), np.arange(1, 6, dtype=np.uint32))
+    s, d, _ = _both_dirs(path)
+    assert gpu_ctx.solve(tri, gpu_ctx.graph_from_edges(6, s, d)) == 0
+    # query larger than the data graph
+    big = gpu_ctx.file_parse(_g("queries/_5_plus"))
+    k3 = synth.UGraph(3, np.array([0, 0, 1], np.uint32), np.array([1, 2, 2], np.uint32))
+    s, d, _ = _both_dirs(k3)
+    assert gpu_ctx.solve(big, gpu_ctx.graph_from_edges(3, s, d)) == 0
+    # isolated vertices in the data graph
+    s, d, _ = _both_dirs(k3)
+    assert gpu_ctx.solve(tri, gpu_ctx.graph_from_edges(50, s, d)) == 6
+    # an edge label the data does not have
+    q = gpu_ctx.parse_text("t # 0\n3 6 1 1\nv 0 1\nv 1 1\nv 2 1\ne 0 1 2\ne 1 0 2\ne 1 2 2\ne 2 1 2\ne 2 0 2\ne 0 2 2\nt # -1")
+    assert gpu_ctx.solve(q, gpu_ctx.graph_from_edges(3, s, d)) == 0
+    # a vertex label the data does not have (vertex-label mode)
+    qv = gpu_ctx_vl.parse_text("t # 0\n3 6 1 1\nv 0 9\nv 1 9\nv 2 9\ne 0 1 1\ne 1 0 1\ne 1 2 1\ne 2 1 1\ne 2 0 1\ne 0 2 1\nt # -1")
+    assert gpu_ctx_vl.solve(qv, gpu_ctx_vl.graph_from_edges(3, s, d)) == 0
+
+
+def test_duplicate_entries_and_self_loops(gpu_ctx, tmp_path):
+    """Duplicate data entries yield duplicate embeddings and data self-loops
+    are rejected by injectivity -- the reference's semantics (HnGPU.cu:168-175,
+    223-236), checked against the oracle's restatement."""
+    rng = np.random.default_rng(5)
+    g = synth.er(80, 6.0, seed=21)
+    s, d = g.directed()
+    extra = rng.integers(0, len(s), 40)
+    loops = rng.integers(0, g.n, 10).astype(np.uint32)
+    s = np.concatenate([s, s[extra], loops]).astype(np.uint32)
+    d = np.concatenate([d, d[extra], loops]).astype(np.uint32)
+    lines = ["t # 0", f"{g.n} {len(s)} 1 1"] + [f"v {i} 1" for i in range(g.n)]
+    lines += [f"e {a} {b} 1" for a, b in zip(s, d)]
+    p = tmp_path / "dup.g"
+    p.write_text("\n".join(lines) + "\nt # -1")
+    od = O.Graph(path=str(p))
+    dev = gpu_ctx.file_parse(str(p))
+    assert dev.to_device().info()["multi_edges"] == 1
+    for qn in ("_3_triangle", "_4_square", "_4_roadY"):
+        oq = O.Graph(path=_g("queries/" + qn))
+        want = O.ffs_count(oq, O.Plan(oq), od, threads=8)
+        assert gpu_ctx.solve(gpu_ctx.file_parse(_g("queries/" + qn)), dev) == want
+
+
+def test_device_ccsr_matches_reference_layout(gpu_ctx):
+    """The device builder reproduces the reference CCSR (row order, rows sorted
+    by target, staggers) recorded from the reference's own fileParse."""
+    ref = json.load(open(os.path.join(GOLD, "ref_frontend.json")))
+    for name in ("data/er200", "data/ba300", "data/grid15", "data/er150_lab3"):
+        r = ref[name]
+        g = gpu_ctx.file_parse(_g(name))
+        rowptr, adj, elab, order = g.download()
+        # rebuild the packed reference segments from the device arrays
+        rows = int(np.count_nonzero(np.diff(rowptr.astype(np.int64))))
+        deg = np.diff(rowptr.astype(np.int64))
+        rowoff = np.concatenate([[0], np.cumsum(deg[:rows] + 1)])[:rows]
+        seg = []
+        for i in range(rows):
+            seg.append(int(deg[i]))
+            for j in range(rowptr[i], rowptr[i + 1]):
+                seg.append(int(rowoff[adj[j]]) | (int(elab[j]) << 24))
+        assert seg == r["segments"]
+        assert order.tolist() == r["inv"]
+
+
+@pytest.mark.parametrize("limits", [
+    dict(mem_limit=64 << 20),
+    dict(max_scan_size=4096),
+    dict(max_soln_size=2048, max_scan_size=8192),
+])
+def test_forced_chunking(tmp_path, limits):
+    """MEMLIMIT-bounded chunking: tiny limits force many steps and retries
+    and must not change any count."""
+    ctx = gfsm_b200.GFSM(device=0, **limits)
+    g = synth.ba(3000, 4, seed=2)
+    s, d, _ = _both_dirs(g)
+    data = ctx.graph_from_edges(g.n, s, d)
+    dpath = tmp_path / "d.g"
+    g.write_text(str(dpath))
+    od = O.Graph(path=str(dpath))
+    for qn in ("_3_triangle", "_4_square", "_4_road4", "_5_plus"):
+        oq = O.Graph(path=_g("queries/" + qn))
+        want = O.ffs_count(oq, O.Plan(oq), od, threads=8)
+        plan = ctx.pre_process_query(ctx.file_parse(_g("queries/" + qn)))
+        got, st = ctx.match_count(plan, data)
+        assert got == want
+        assert st["steps"] > 3
+    ctx.close()
+
+
+def test_batch_equals_one_at_a_time(gpu_ctx_vl):
+    g = synth.rmat(12, 30000, seed=4)
+    g.vlabel = synth.vlabels(g.n, 4, 0.0, seed=5)
+    s, d, _ = _both_dirs(g)
+    data = gpu_ctx_vl.graph_from_edges(g.n, s, d, None, g.vlabel)
+    plans = []
+    for i in range(64):
+        qg, _ = synth.rw_query(g, 3 + i % 6, tree=i % 2 == 0, seed=i)
+        qs, qd = qg.directed()
+        q = gpu_ctx_vl.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)
+        plans.append(gpu_ctx_vl.pre_process_query(q))
+    batch, st = gpu_ctx_vl.batch_count(plans, data)
+    single = [gpu_ctx_vl.match_count(p, data)[0] for p in plans]
+    assert batch.tolist() == single
+    assert sum(single) > 0
+
+
+def test_full_size_rmat(gpu_ctx):
+    """Size-independent properties at the R-MAT 2^20 (~16M edges) size: the
+    counts of an edge and of a 3-path are closed forms of the degree sequence,
+    and the triangle count is 6x the triangles found by an independent
+    orientation-and-intersection counter."""
+    g = synth.rmat(20, 16 << 20, seed=0)
+    s, d, _ = _both_dirs(g)
+    data = gpu_ctx.graph_from_edges(g.n, s, d)
+    deg = np.bincount(np.concatenate([g.src, g.dst]), minlength=g.n).astype(object)
+    q2 = gpu_ctx.file_parse(_g("queries/_2_road2"))
+    assert gpu_ctx.solve(q2, data) == 2 * g.m
+    q3 = gpu_ctx.file_parse(_g("queries/_3_road3"))
+    assert gpu_ctx.solve(q3, data) == int(sum(x * (x - 1) for x in deg))
+    tri = gpu_ctx.file_parse(_g("queries/_3_triangle"))
+    assert gpu_ctx.solve(tri, data) == 6 * O.triangles(g.n, g.src, g.dst)
+
+
+def test_triangles_medium_rmat(gpu_ctx):
+    g = synth.rmat(14, 200_000, seed=1)
+    s, d, _ = _both_dirs(g)
+    data = gpu_ctx.graph_from_edges(g.n, s, d)
+    tri = gpu_ctx.file_parse(_g("queries/_3_triangle"))
+    assert gpu_ctx.solve(tri, data) == 6 * O.triangles(g.n, g.src, g.dst)

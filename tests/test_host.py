@@ -1,0 +1,122 @@
+"""CPU tests of the product's host side through the C ABI: the library loads
+and exports every symbol include/gfsm.h declares; the multi-threaded parser
+and the planner reproduce the reference's front-end (pinned fixtures); error
+codes match the reference's exit codes.  No kernel runs here."""
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import gfsm_b200
+from gfsm_b200 import _lib
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+REF = json.load(open(os.path.join(GOLD, "ref_frontend.json")))
+
+
+def test_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "gfsm.h")).read()
+    declared = set(re.findall(r"\b(gfsm_[a-z_]+)\s*\(", hdr))
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (gfsm_[a-z_]+)", out))
+    assert declared, "no declarations found"
+    assert declared <= exported, declared - exported
+    assert declared == set(_lib.SIGNATURES), set(_lib.SIGNATURES) ^ declared
+    _lib.load()
+
+
+def test_cli_binary_links():
+    r = subprocess.run(["ldd", os.path.join(ROOT, "gfsm_b200", "GFSM")], capture_output=True, text=True)
+    assert "libgfsm.so" in r.stdout and "not found" not in r.stdout
+
+
+def test_limits_defaults_are_environment_h(monkeypatch):
+    for k in ("GFSM_MEMLIMIT", "GFSM_MAXSOLNSIZE", "GFSM_MAXSCANSIZE", "GFSM_CCSRRELSIZE", "GFSM_UPPERMEMLIMIT"):
+        monkeypatch.delenv(k, raising=False)
+    lim = gfsm_b200.default_limits()
+    assert lim.ccsr_rel_size == 8
+    assert lim.max_soln_size == 500_000_000 and lim.max_scan_size == 500_000_000
+    assert lim.mem_limit == 22_000_000_000 and lim.upper_mem_limit == 44_000_000_000
+    assert lim.vertex_labels == 0
+    monkeypatch.setenv("GFSM_MEMLIMIT", "1e9")
+    assert gfsm_b200.default_limits().mem_limit == 1_000_000_000
+
+
+@pytest.mark.parametrize("key", sorted(k for k in REF if k.startswith("queries/")))
+def test_planner_matches_reference(host_ctx, key):
+    r = REF[key]
+    q = host_ctx.file_parse(os.path.join(GOLD, key + ".g"))
+    t = host_ctx.pre_process_query(q).tables()
+    assert t["max_valency"] == r["max_valency"]
+    assert t["reqs"].tolist() == r["reqs"]
+    assert t["header"].tolist() == r["header"]
+
+
+def test_planner_matches_oracle_on_random_walks(host_ctx, tmp_path):
+    from gfsm_b200 import synth
+    g = synth.ba(2000, 3, seed=5)
+    for i in range(40):
+        k = 3 + i % 10
+        qg, _ = synth.rw_query(g, k, tree=i % 3 == 0, seed=i)
+        p = tmp_path / f"q{i}.g"
+        qg.write_text(str(p))
+        mine = host_ctx.pre_process_query(host_ctx.file_parse(str(p))).tables()
+        ref = O.Plan(O.Graph(path=str(p))).tables()
+        assert mine["reqs"].tolist() == ref["reqs"].tolist()
+        assert mine["header"].tolist() == ref["header"].tolist()
+        assert mine["order"].tolist() == ref["order"].tolist()
+
+
+def test_parser_error_codes(host_ctx, tmp_path):
+    cases = {
+        "t # 1\n1 0 1 1\nt # -1": 233,
+        "t # 0\n3 2 1 1\nv 0 1\nt # -1": 234,
+        "t # 0\n2 4 1 1\nv 0 1\nv 1 1\ne 0 1 1\ne 1 0 1\nt # -1": 234,
+        "t # 0\n2 2 1 1\nv 0 1\nx 1 1\nt # -1": 233,
+        "t # 0\n2 2 1 1\nv 0 1\ne 0 1 1\nv 1 1\nt # -1": 233,
+        "t # 0\n2 2 1 1\nv 0 1\ne 0 5 1\ne 1 0 1\nt # -1": 233,
+    }
+    for text, code in cases.items():
+        with pytest.raises(gfsm_b200.GFSMError) as ei:
+            host_ctx.parse_text(text)
+        assert ei.value.status == code, text
+        p = tmp_path / "x.g"
+        p.write_text(text)
+        assert O.Graph(path=str(p)).err == code or code == 233
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.file_parse(str(tmp_path / "nope.g"))
+    assert ei.value.status == 232
+
+
+def test_parser_large_multichunk_matches_oracle(host_ctx, tmp_path):
+    """A file big enough to be split across threads parses to the same edges."""
+    from gfsm_b200 import synth
+    g = synth.rmat(15, 120_000, seed=3)
+    p = tmp_path / "big.g"
+    g.write_text(str(p))
+    assert os.path.getsize(p) > 3 << 20
+    dg = host_ctx.file_parse(str(p))
+    info = dg.info()
+    og = O.Graph(path=str(p))
+    assert info["n"] == og.arrays()["count"] and info["m"] == 2 * g.m
+    assert info["rows"] == og.arrays()["rows"]
+
+
+def test_disconnected_query_is_status_1(host_ctx):
+    q = host_ctx.parse_text("t # 0\n4 4 1 1\nv 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 1 0 1\ne 2 3 1\ne 3 2 1\nt # -1")
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.pre_process_query(q)
+    assert ei.value.status == 1
+
+
+def test_matching_needs_a_device(host_ctx):
+    q = host_ctx.file_parse(os.path.join(GOLD, "queries", "_3_triangle.g"))
+    d = host_ctx.file_parse(os.path.join(GOLD, "data", "er200.g"))
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.solve(q, d)
+    assert ei.value.status == 305

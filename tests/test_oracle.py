@@ -1,0 +1,182 @@
+"""CPU tests of the oracle: pinned to the reference's own front-end output
+(tests/golden/ref_frontend.json, produced by the reference's fileParse /
+preProcessQuery), to closed-form counts, and to agreement between the FFS
+restatement and the independent backtracking enumerator."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from gfsm_b200 import synth
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF = json.load(open(os.path.join(GOLD, "ref_frontend.json")))
+COUNTS = json.load(open(os.path.join(GOLD, "counts.json")))
+
+
+def _gfile(key):
+    return os.path.join(GOLD, key + ".g")
+
+
+@pytest.mark.parametrize("key", sorted(REF))
+def test_oracle_parse_matches_reference(key):
+    r = REF[key]
+    g = O.Graph(path=_gfile(key))
+    assert g.err == 0
+    a = g.arrays()
+    assert a["count"] == r["count"] and a["size"] == r["size"]
+    assert g.packed().tolist() == r["segments"]
+    assert a["vlocs"].tolist() == r["vlocs"]
+    assert a["inv"].tolist() == r["inv"]
+    assert a["staggers"].tolist() == r["staggers"]
+    assert a["sinfo"].tolist() == r["sinfo"]
+
+
+@pytest.mark.parametrize("key", sorted(k for k in REF if k.startswith("queries/")))
+def test_oracle_plan_matches_reference(key):
+    r = REF[key]
+    t = O.Plan(O.Graph(path=_gfile(key))).tables()
+    assert t["max_valency"] == r["max_valency"]
+    assert t["reqs"].tolist() == r["reqs"]
+    assert t["header"].tolist() == r["header"]
+
+
+@pytest.mark.parametrize("key", sorted(COUNTS))
+def test_oracle_golden_counts(key):
+    qn, dn = key.split("|")
+    q = O.Graph(path=_gfile("queries/" + qn))
+    d = O.Graph(path=_gfile("data/" + dn))
+    p = O.Plan(q)
+    assert O.ffs_count(q, p, d, threads=4) == COUNTS[key]["count"]
+    assert O.ffs_count(q, p, d, vlabel_mode=True, threads=4) == COUNTS[key]["count_vlabels"]
+
+
+def _complete(n):
+    s, d = np.triu_indices(n, 1)
+    return synth.UGraph(n, s.astype(np.uint32), d.astype(np.uint32))
+
+
+def _text(g, tmp_path, name, lab=None):
+    p = tmp_path / name
+    g.write_text(str(p), lab)
+    return O.Graph(path=str(p))
+
+
+def test_closed_forms(tmp_path):
+    # triangle on K_n: n(n-1)(n-2); K_{1,4} ("plus") on a star K_{1,m}: m(m-1)(m-2)(m-3);
+    # a k-vertex path on the cycle C_n: 2n
+    tri = O.Graph(path=_gfile("queries/_3_triangle"))
+    for n in (3, 4, 7, 10):
+        d = _text(_complete(n), tmp_path, f"k{n}.g")
+        assert O.ffs_count(tri, O.Plan(tri), d) == n * (n - 1) * (n - 2)
+    plus = O.Graph(path=_gfile("queries/_5_plus"))
+    for m in (4, 6, 9):
+        star = synth.UGraph(m + 1, np.zeros(m, np.uint32), np.arange(1, m + 1, dtype=np.uint32))
+        d = _text(star, tmp_path, f"s{m}.g")
+        assert O.ffs_count(plus, O.Plan(plus), d) == m * (m - 1) * (m - 2) * (m - 3)
+    for k, qn in ((2, "_2_road2"), (3, "_3_road3"), (4, "_4_road4"), (5, "_5_road5")):
+        q = O.Graph(path=_gfile("queries/" + qn))
+        for n in (k if k > 2 else 3, 8, 13):
+            if n < k:
+                continue
+            cyc = synth.UGraph(n, np.arange(n, dtype=np.uint32), (np.arange(n, dtype=np.uint32) + 1) % n)
+            cyc.src, cyc.dst = np.minimum(cyc.src, cyc.dst), np.maximum(cyc.src, cyc.dst)
+            d = _text(cyc, tmp_path, f"c{n}.g")
+            expect = 2 * n if not (k == n == 3) else 6
+            assert O.ffs_count(q, O.Plan(q), d) == expect
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_ffs_matches_backtracking(seed, tmp_path):
+    gen = [lambda: synth.er(120, 5.0, seed=seed), lambda: synth.ba(150, 2, seed=seed),
+           lambda: synth.grid(10, 0.1, 0.05, seed=seed)][seed % 3]
+    g = gen()
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=seed + 50)
+    lab = (np.arange(g.m, dtype=np.uint32) * 7 + seed) % 2 + 1 if seed % 2 else None
+    d = _text(g, tmp_path, "d.g", lab)
+    ds, dd, dl = d.edges()
+    for k in (3, 4, 5):
+        for tree in (False, True):
+            qg, visited = synth.rw_query(g, k, tree=tree, seed=100 * seed + k)
+            qlab = None
+            if lab is not None:
+                key = {(int(a), int(b)): int(l) for a, b, l in zip(g.src, g.dst, lab)}
+                qlab = np.array([key[(min(visited[a], visited[b]), max(visited[a], visited[b]))]
+                                 for a, b in zip(qg.src, qg.dst)], np.uint32)
+            q = _text(qg, tmp_path, "q.g", qlab)
+            p = O.Plan(q)
+            assert p.err == 0
+            qs, qd, ql = q.edges()
+            for vl in (False, True):
+                c1 = O.ffs_count(q, p, d, vlabel_mode=vl, threads=2)
+                c2 = O.bt_count(k, qs, qd, ql, q.arrays()["vlabel"], g.n, ds, dd, dl, d.arrays()["vlabel"],
+                                vlabel_mode=vl, threads=2)
+                assert c1 == c2 and c1 >= (1 if not vl else 0)
+
+
+def test_mappings_agree(tmp_path):
+    g = synth.er(60, 5.0, seed=3)
+    d = _text(g, tmp_path, "d.g")
+    q = O.Graph(path=_gfile("queries/_4_square"))
+    p = O.Plan(q)
+    c1, r1 = O.ffs_count(q, p, d, max_rows=100000)
+    qs, qd, ql = q.edges()
+    ds, dd, dl = d.edges()
+    c2, r2 = O.bt_count(4, qs, qd, ql, None, g.n, ds, dd, dl, None, max_rows=100000)
+    assert c1 == c2 == len(r1) == len(r2)
+    s1 = r1[np.lexsort(r1.T[::-1])]
+    s2 = r2[np.lexsort(r2.T[::-1])]
+    assert np.array_equal(s1, s2)
+
+
+def test_parser_error_codes(tmp_path):
+    (tmp_path / "bad.g").write_text("t # 1\n1 0 1 1\nt # -1")
+    assert O.Graph(path=str(tmp_path / "bad.g")).err == 233
+    assert O.Graph(path=str(tmp_path / "missing.g")).err == 232
+    (tmp_path / "few.g").write_text("t # 0\n3 2 1 1\nv 0 1\nt # -1")
+    assert O.Graph(path=str(tmp_path / "few.g")).err == 234
+    (tmp_path / "fewe.g").write_text("t # 0\n2 4 1 1\nv 0 1\nv 1 1\ne 0 1 1\ne 1 0 1\nt # -1")
+    assert O.Graph(path=str(tmp_path / "fewe.g")).err == 234
+    (tmp_path / "junk.g").write_text("t # 0\n2 2 1 1\nv 0 1\nx 1 1\nt # -1")
+    assert O.Graph(path=str(tmp_path / "junk.g")).err == 233
+
+
+def test_disconnected_query_rejected(tmp_path):
+    (tmp_path / "dq.g").write_text("t # 0\n4 4 1 1\nv 0 1\nv 1 1\nv 2 1\nv 3 1\n"
+                                   "e 0 1 1\ne 1 0 1\ne 2 3 1\ne 3 2 1\nt # -1")
+    q = O.Graph(path=str(tmp_path / "dq.g"))
+    assert O.Plan(q).err == 1
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_FRONTEND), reason="reference front-end not built here")
+def test_reference_frontend_live(tmp_path):
+    """Live comparison with the reference's own parser/planner on fresh inputs,
+    including its parser's error exits."""
+    for seed in range(4):
+        g = synth.ba(80 + seed * 30, 2 + seed % 3, seed=seed)
+        p = tmp_path / f"g{seed}.g"
+        g.write_text(str(p))
+        rc, r = O.ref_frontend_dump(str(p))
+        d = O.Graph(path=str(p))
+        assert rc == 0 and d.packed().tolist() == r["segments"].tolist()
+        assert d.arrays()["sinfo"].tolist() == r["sinfo"].tolist()
+        qg, _ = synth.rw_query(g, 6, tree=seed % 2 == 0, seed=seed)
+        qp = tmp_path / f"q{seed}.g"
+        qg.write_text(str(qp))
+        rc, r = O.ref_frontend_dump(str(qp), plan=True)
+        t = O.Plan(O.Graph(path=str(qp))).tables()
+        assert rc == 0 and t["reqs"].tolist() == r["reqs"].tolist() and t["header"].tolist() == r["header"].tolist()
+    (tmp_path / "few.g").write_text("t # 0\n3 2 1 1\nv 0 1\nt # -1")
+    assert O.ref_frontend_dump(str(tmp_path / "few.g"))[0] == 234
+    (tmp_path / "bad.g").write_text("t # 1\n1 0 1 1\nt # -1")
+    assert O.ref_frontend_dump(str(tmp_path / "bad.g"))[0] == 233
+    # the shipped sample queries parse and plan exactly like our fixtures of the same shapes
+    for f in glob.glob("/root/reference/build/query/*.g"):
+        name = os.path.basename(f)[:-2]
+        rc, r = O.ref_frontend_dump(f, plan=True)
+        assert rc == 0
+        assert r["segments"].tolist() == REF["queries/" + name]["segments"]
+        assert r["reqs"].tolist() == REF["queries/" + name]["reqs"]
