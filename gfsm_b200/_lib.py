@@ -80,7 +80,10 @@ class Stats(C.Structure):
         ("retries", C.c_uint64),
         ("peak_frontier_bytes", C.c_uint64),
         ("kernel_ms", C.c_double),
+        ("device_ms", C.c_double),
         ("wall_ms", C.c_double),
+        ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64),
     ]
 
     def as_dict(self):

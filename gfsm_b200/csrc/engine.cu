@@ -514,11 +514,13 @@ void Engine::release() {
     if (h_result) cudaFreeHost(h_result);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_begin) cudaEventDestroy(ev_begin);
+    if (ev_end) cudaEventDestroy(ev_end);
     if (stream) cudaStreamDestroy(stream);
     arena = nullptr;
     small = nullptr;
     h_result = nullptr;
-    ev0 = ev1 = nullptr;
+    ev0 = ev1 = ev_begin = ev_end = nullptr;
     stream = nullptr;
 }
 
@@ -528,6 +530,8 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     ECHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     ECHECK(cudaEventCreate(&ev0));
     ECHECK(cudaEventCreate(&ev1));
+    ECHECK(cudaEventCreate(&ev_begin));
+    ECHECK(cudaEventCreate(&ev_end));
     ECHECK(cudaMallocHost(&h_result, sizeof(StepResult)));
     max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
     status_tiles = (uint32_t)div_up(max_scan, TILE);
@@ -628,6 +632,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)na + 1) * 8, cudaMemcpyHostToDevice, stream));
     ECHECK(cudaMemcpyAsync(d_rcstart, rlo.data(), (uint64_t)na * 4, cudaMemcpyHostToDevice, stream));
     ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
+    st.h2d_bytes += plans_bytes + ((uint64_t)na + 1) * 8 + (uint64_t)na * 4;
+    ECHECK(cudaEventRecord(ev_begin, stream));
 
     // depth buffers 0 .. dmax-1 (depth dmax is count-only)
     const uint64_t rest = budget - (uint64_t)(p - static_cast<char *>(arena));
@@ -639,7 +645,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     };
     std::vector<Buf> buf(dmax);
     {
-        const uint64_t share = dmax ? rest / dmax : 0;
+        // every depth buffer starts on a 256-byte boundary (u64 coff arrays)
+        const uint64_t share = dmax ? (rest / dmax) & ~255ull : 0;
         for (uint32_t d = 0; d < dmax; ++d) {
             const uint64_t per = 4ull * (d + 2) + 4 + 8;
             uint64_t cap = share > 1024 ? (share - 1024) / per : 0;
@@ -654,6 +661,11 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             b.tup = reinterpret_cast<uint32_t *>(q);
             q += (cap * 4 * (d + 2) + 255) & ~255ull;
             b.cstart = reinterpret_cast<uint32_t *>(q);
+            if ((reinterpret_cast<uintptr_t>(b.coff) | reinterpret_cast<uintptr_t>(b.tup) |
+                 reinterpret_cast<uintptr_t>(b.cstart)) & 255u) {
+                err = "frontier buffer not 256-byte aligned";
+                return GFSM_ERR_CUDA;
+            }
         }
         st.peak_frontier_bytes = budget;
     }
@@ -726,6 +738,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         ECHECK(cudaEventRecord(ev1, stream));
         ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
         ECHECK(cudaStreamSynchronize(stream));
+        st.d2h_bytes += sizeof(StepResult);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         kms += ms;
@@ -756,8 +769,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             }
         }
     }
+    ECHECK(cudaEventRecord(ev_end, stream));
     std::vector<unsigned long long> cnt(na);
     ECHECK(cudaMemcpyAsync(cnt.data(), d_counts, (uint64_t)na * 8, cudaMemcpyDeviceToHost, stream));
+    st.d2h_bytes += (uint64_t)na * 8;
     if (rows_out) ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
     ECHECK(cudaStreamSynchronize(stream));
     for (uint32_t i = 0; i < na; ++i) counts_out[active[i]] = cnt[i];
@@ -766,10 +781,16 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         for (uint32_t i = 0; i < na; ++i) total_rows += cnt[i];
         const uint64_t nr = std::min<uint64_t>(total_rows, max_rows);
         if (nr) ECHECK(cudaMemcpy(rows_out, d_rows, nr * dq[0].k * 4, cudaMemcpyDeviceToHost));
+        st.d2h_bytes += nr * dq[0].k * 4;
         if (n_rows) *n_rows = nr;
     }
     for (uint32_t i = 0; i < na; ++i) st.count += cnt[i];
     st.kernel_ms = kms;
+    {
+        float dms = 0.f;
+        cudaEventElapsedTime(&dms, ev_begin, ev_end);
+        st.device_ms = dms;
+    }
     st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     if (stats) *stats = st;
     return GFSM_OK;

@@ -12,7 +12,7 @@ namespace gfsm {
 struct Engine {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_begin = nullptr, ev_end = nullptr;
     void *arena = nullptr;         // frontier buffers + per-call plans/counts
     uint64_t arena_bytes = 0;
     uint64_t arena_cap = 0;        // bytes the arena may use (MEMLIMIT share)

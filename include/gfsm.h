@@ -79,8 +79,11 @@ typedef struct {
     uint64_t steps;              /* frontier steps launched                        */
     uint64_t retries;            /* steps re-run with a smaller chunk              */
     uint64_t peak_frontier_bytes;/* device bytes of the frontier arena in use     */
-    double   kernel_ms;          /* device time of the matching kernels            */
+    double   kernel_ms;          /* device time of the level-step kernels (sum)    */
+    double   device_ms;          /* device timeline of the call: first step to last */
     double   wall_ms;            /* host wall time of the call                     */
+    uint64_t h2d_bytes;          /* host->device bytes copied by the call          */
+    uint64_t d2h_bytes;          /* device->host bytes copied by the call          */
 } gfsm_stats;
 
 typedef struct {
