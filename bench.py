@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark: queries/s and p99 latency, batched vs plain, with exact counts.
+
+Workload (default): the served / batched configuration -- a 1,400 x 1,400
+road-like grid (5% of edges removed, 2% random long-range shortcuts, 4
+uniform vertex labels, vertex labels matched), resident on the device, and a
+batch of 4,096 seeded random-walk queries of 4-10 vertices (all induced
+edges).  One step = the whole batch through gfsm_batch_count.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Reported on one JSON line (rank 0):
+  value      batched queries/s on the device timeline (inputs resident)
+  e2e        the same through the C ABI from host edge lists: query graphs
+             built + planned on the host, plans copied in, counts copied out
+  plain      one-query-at-a-time queries/s and latency percentiles
+  served     Poisson arrivals at 100 / 1,000 / 10,000 queries/s: p50 / p99
+  roofline   level-step kernel: algorithmic bytes / kernel time vs HBM peak
+  cpu_baseline  the oracle's restatement of the reference algorithm on the
+             host cores over a bounded sample of the same queries
+With N > 1 every rank runs its own batch (weak scaling, no collective on the
+data path); value = all ranks' queries / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID_SIDE = 1400
+NQ = 4096
+KMIN, KMAX = 4, 10
+SERVE_RATES = (100, 1000, 10000)
+WORKLOAD = ("config5 road-like grid 1400x1400 (5% edges removed, 2% shortcuts, 4 uniform vertex labels, "
+            "vertex labels matched), 4096 random-walk queries of 4-10 vertices with all induced edges")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--queries", type=int, default=NQ)
+    ap.add_argument("--no-serve", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x, local):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x, local):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_workload(rank, nq):
+    from gfsm_b200 import synth
+    g = synth.grid(GRID_SIDE, 0.05, 0.02, seed=0)
+    g.vlabel = synth.vlabels(g.n, 4, 0.0, seed=100)
+    rng = np.random.default_rng(11 + rank)
+    qs = []
+    for i in range(nq):
+        k = int(rng.integers(KMIN, KMAX + 1))
+        q, _ = synth.rw_query(g, k, tree=False, seed=1 + i + 1_000_003 * rank)
+        qs.append(q)
+    return g, qs
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join("/tmp", f"gfsm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def traffic_record():
+    """Measured DRAM bytes per level-step launch from a committed ncu summary, if any."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except Exception:
+        return None
+
+
+class CpuOracle:
+    """The oracle's restatement of the reference's FFS algorithm on the host
+    cores (all threads), over the same data graph and queries."""
+
+    def __init__(self, g, threads=None):
+        import tempfile
+
+        from oracle import oracle
+        self.oracle = oracle
+        self.threads = threads or os.cpu_count() or 1
+        self.tmp = tempfile.mkdtemp()
+        dpath = os.path.join(self.tmp, "d.g")
+        g.write_text(dpath)
+        self.od = oracle.Graph(path=dpath)
+
+    def run(self, qs, budget_s):
+        """Queries from the front of qs until budget_s is spent."""
+        o = self.oracle
+        done, counts = 0, []
+        t0 = time.perf_counter()
+        for q in qs:
+            qp = os.path.join(self.tmp, "q.g")
+            q.write_text(qp)
+            oq = o.Graph(path=qp)
+            counts.append(o.ffs_count(oq, o.Plan(oq), self.od, vlabel_mode=True, threads=self.threads))
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        return done, time.perf_counter() - t0, counts
+
+
+def run_reference(args, rank, world, pg):
+    if rank != 0:
+        return
+    g, qs = make_workload(0, args.queries)
+    cpu = CpuOracle(g)
+    threads = cpu.threads
+    per_step = []
+    total_q = 0
+    for i in range(args.warmup + args.steps):
+        done, el, _ = cpu.run(qs, budget_s=8.0)
+        if i >= args.warmup:
+            per_step.append((done, el))
+            total_q += done
+    el = sum(e for _, e in per_step)
+    qps = total_q / el if el else 0.0
+    line = {
+        "impl": "reference", "metric": "queries/s (batched, exact counts)", "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / len(per_step),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "queries_per_step": args.queries},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"first queries of the batch, ~8 s of CPU per step ({total_q} queries timed)"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local, pg):
+    import gfsm_b200
+    ctx = gfsm_b200.GFSM(device=local, vertex_labels=1)
+    g, qs = make_workload(rank, args.queries)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel).to_device()
+    qdir = [(q.n,) + tuple(q.directed()) + (q.vlabel,) for q in qs]
+
+    def plans_from_host():
+        out = []
+        for n, a, b, vl in qdir:
+            qg = ctx.graph_from_edges(n, a, b, None, vl)
+            out.append(ctx.pre_process_query(qg))
+        return out
+
+    plans = plans_from_host()
+    import torch
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def flush_l2():
+        flush_buf.fill_(1)
+        torch.cuda.synchronize(local)
+
+    for _ in range(args.warmup):
+        counts, st = ctx.batch_count(plans, data)
+    ref_counts = counts.copy()
+
+    # -- device-resident batched steps
+    clocks = Clocks(local)
+    dev_ms, k_ms, alg, launches, cand = [], 0.0, 0, 0, 0
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    for _ in range(args.steps):
+        flush_l2()
+        counts, st = ctx.batch_count(plans, data)
+        assert counts.tolist() == ref_counts.tolist()
+        dev_ms.append(st["device_ms"])
+        k_ms += st["kernel_ms"]
+        alg += st["alg_bytes"]
+        launches += 2 * st["steps"]
+        cand += st["candidates"]
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    clk = clocks.stop()
+    t_dev = max_over_ranks(pg, sum(dev_ms) / 1000.0, local)
+    total_queries = sum_over_ranks(pg, float(args.queries * args.steps), local)
+    value = total_queries / t_dev
+
+    # -- end to end through the C ABI from host buffers
+    barrier(pg)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        p2 = plans_from_host()
+        counts2, st2 = ctx.batch_count(p2, data)
+        h2d += st2["h2d_bytes"]
+        d2h += st2["d2h_bytes"]
+        for p in p2:
+            p.close()
+    t_e2e = max_over_ranks(pg, time.perf_counter() - t0, local)
+    assert counts2.tolist() == ref_counts.tolist()
+    e2e = total_queries / t_e2e
+
+    # -- plain form: one query at a time
+    lat = []
+    t0 = time.perf_counter()
+    plain_counts = []
+    for p in plans:
+        a = time.perf_counter()
+        c, _ = ctx.match_count(p, data)
+        lat.append((time.perf_counter() - a) * 1000.0)
+        plain_counts.append(c)
+    t_plain = time.perf_counter() - t0
+    exact = plain_counts == ref_counts.tolist()
+    lat.sort()
+    plain = {"queries_per_s": len(plans) / t_plain, "p50_ms": lat[len(lat) // 2], "p99_ms": lat[int(len(lat) * 0.99)],
+             "queries": len(plans)}
+
+    # -- served form: Poisson arrivals
+    served = {}
+    if not args.no_serve:
+        rng = np.random.default_rng(5)
+        for rate in SERVE_RATES:
+            n = min(len(plans), max(200, int(rate * 2.0)))
+            srv = ctx.serve(data, slots=2, max_batch=256)
+            gaps = rng.exponential(1.0 / rate, n)
+            t0 = time.perf_counter()
+            nxt = t0
+            for i in range(n):
+                nxt += gaps[i]
+                while True:
+                    now = time.perf_counter()
+                    if now >= nxt:
+                        break
+                    time.sleep(min(nxt - now, 0.001))
+                srv.submit(plans[i], i)
+            srv.drain(120000)
+            wall = time.perf_counter() - t0
+            res = srv.poll(n + 10)
+            srv.stop()
+            ls = sorted(r["done_ms"] - r["submit_ms"] for r in res)
+            ok = all(r["count"] == ref_counts[r["req_id"]] for r in res) and len(res) == n
+            exact = exact and ok
+            served[str(rate)] = {"offered_qps": rate, "queries": n, "achieved_qps": n / wall,
+                                 "p50_ms": ls[len(ls) // 2], "p99_ms": ls[int(len(ls) * 0.99)]}
+
+    # -- roofline of the level-step kernel
+    pk, pk_kind = peaks()
+    achieved = alg / (k_ms / 1000.0) / 1e9 if k_ms else 0.0
+    tr = traffic_record()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": tr.get("bytes_per_launch") if tr else None,
+            "peak_source": pk_kind, "kernel": "k_step (level step)",
+            "alg_bytes_per_step": alg / args.steps, "kernel_ms_per_step": k_ms / args.steps,
+            "candidates_per_s": cand / (k_ms / 1000.0) if k_ms else 0.0}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        co = CpuOracle(g)
+        done, el, ccounts = co.run(qs, budget_s=15.0)
+        exact = exact and ccounts == ref_counts[:done].tolist()
+        cpu = {"value": done / el, "unit": "queries/s", "cores": co.threads, "kind": "port",
+               "sample": f"first {done} queries of the batch (~15 s of host CPU), oracle restatement of the "
+                         f"reference FFS algorithm"}
+
+    if rank == 0:
+        line = {
+            "metric": "queries/s (batched, exact counts) with p99 latency; plain and served beside it",
+            "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "queries_per_step": args.queries, "vertex_labels": True,
+                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}"},
+            "exact": exact, "batched_over_plain": value / plain["queries_per_s"],
+            "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    rank, world, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, pg)
+        else:
+            run_ours(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -53,6 +53,7 @@ class Limits(C.Structure):
         ("upper_mem_limit", C.c_uint64),
         ("vertex_labels", C.c_int32),
         ("degree_filter", C.c_int32),
+        ("max_candidates", C.c_uint64),
     ]
 
 

@@ -86,6 +86,7 @@ void gfsm_limits_default(gfsm_limits *lim) {
     lim->mem_limit = env_u64("GFSM_MEMLIMIT", kMemLimit);
     lim->vertex_labels = (int32_t)env_u64("GFSM_VERTEX_LABELS", 0);
     lim->degree_filter = (int32_t)env_u64("GFSM_DEGREE_FILTER", 1);
+    lim->max_candidates = env_u64("GFSM_MAXCANDIDATES", 0);
 }
 
 const char *gfsm_status_str(gfsm_status s) {

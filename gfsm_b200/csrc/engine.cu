@@ -756,6 +756,11 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
         st.candidates += chunk;
         st.expansions += r.n_children;
+        if (lim.max_candidates && st.candidates > lim.max_candidates) {
+            err = "candidate cap (max_candidates) reached";
+            if (stats) *stats = st;
+            return GFSM_ERR_TOO_LARGE;
+        }
         st.alg_bytes += r.alg_bytes + (emits ? r.n_children * 4ull * (d + 1) : 0ull);
         pos[d] += chunk;
         if (emits) {

@@ -52,6 +52,8 @@ typedef struct {
     int32_t  vertex_labels;    /* 0 = reference semantics (labels ignored), 1 = must match    */
     int32_t  degree_filter;    /* 1 = skip candidates whose degree is below the query degree
                                   (count-preserving; applied only to symmetric graphs)       */
+    uint64_t max_candidates;   /* stop a call with GFSM_ERR_TOO_LARGE once this many
+                                  candidates were examined; 0 = no cap                        */
 } gfsm_limits;
 
 typedef struct gfsm_ctx gfsm_ctx;
