@@ -49,7 +49,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--queries", type=int, default=NQ)
-    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-at-a-time measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     return ap.parse_args()
 
 
@@ -290,19 +292,22 @@ def run_ours(args, rank, world, local, pg):
     e2e = total_queries / t_e2e
 
     # -- plain form: one query at a time
-    lat = []
-    t0 = time.perf_counter()
-    plain_counts = []
-    for p in plans:
-        a = time.perf_counter()
-        c, _ = ctx.match_count(p, data)
-        lat.append((time.perf_counter() - a) * 1000.0)
-        plain_counts.append(c)
-    t_plain = time.perf_counter() - t0
-    exact = plain_counts == ref_counts.tolist()
-    lat.sort()
-    plain = {"queries_per_s": len(plans) / t_plain, "p50_ms": lat[len(lat) // 2], "p99_ms": lat[int(len(lat) * 0.99)],
-             "queries": len(plans)}
+    exact = True
+    plain = None
+    if not args.no_plain:
+        lat = []
+        t0 = time.perf_counter()
+        plain_counts = []
+        for p in plans:
+            a = time.perf_counter()
+            c, _ = ctx.match_count(p, data)
+            lat.append((time.perf_counter() - a) * 1000.0)
+            plain_counts.append(c)
+        t_plain = time.perf_counter() - t0
+        exact = plain_counts == ref_counts.tolist()
+        lat.sort()
+        plain = {"queries_per_s": len(plans) / t_plain, "p50_ms": lat[len(lat) // 2],
+                 "p99_ms": lat[int(len(lat) * 0.99)], "queries": len(plans)}
 
     # -- served form: Poisson arrivals
     served = {}
@@ -336,14 +341,20 @@ def run_ours(args, rank, world, local, pg):
     pk, pk_kind = peaks()
     achieved = alg / (k_ms / 1000.0) / 1e9 if k_ms else 0.0
     tr = traffic_record()
+    k_launches = launches // 2
+    traffic = None
+    if tr and k_launches:
+        # measured DRAM bytes per candidate (small-case ncu capture) x candidates per launch
+        traffic = tr["dram_bytes_per_candidate"] * cand / k_launches
     roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": tr.get("bytes_per_launch") if tr else None,
+            "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+            "alg_bytes_per_launch": alg / k_launches if k_launches else None,
             "peak_source": pk_kind, "kernel": "k_step (level step)",
             "alg_bytes_per_step": alg / args.steps, "kernel_ms_per_step": k_ms / args.steps,
             "candidates_per_s": cand / (k_ms / 1000.0) if k_ms else 0.0}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         co = CpuOracle(g)
         done, el, ccounts = co.run(qs, budget_s=15.0)
         exact = exact and ccounts == ref_counts[:done].tolist()
@@ -359,7 +370,7 @@ def run_ours(args, rank, world, local, pg):
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "queries_per_step": args.queries, "vertex_labels": True,
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}"},
-            "exact": exact, "batched_over_plain": value / plain["queries_per_s"],
+            "exact": exact, "batched_over_plain": value / plain["queries_per_s"] if plain else None,
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
