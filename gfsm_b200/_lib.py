@@ -36,6 +36,7 @@ SIGNATURES = {
     "gfsm_match_count": (C.c_int, [vp, vp, vp, u64p, vp]),
     "gfsm_match_mappings": (C.c_int, [vp, vp, vp, u32p, C.c_uint64, u64p, u64p, vp]),
     "gfsm_batch_count": (C.c_int, [vp, C.POINTER(vp), C.c_int, vp, u64p, vp]),
+    "gfsm_match_count_noalloc": (C.c_int, [vp, vp, vp, u64p]),
     "gfsm_serve_start": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "gfsm_serve_submit": (C.c_int, [vp, vp, C.c_uint64]),
     "gfsm_serve_poll": (C.c_int, [vp, vp, C.c_int, C.POINTER(C.c_int)]),

@@ -31,6 +31,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "engine.h"
 
@@ -802,3 +803,214 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
 }
 
 }  // namespace gfsm
+
+// ---------------------------------------------------------------------------
+// gfsm_match_count_noalloc: the level steps above, run entirely out of one
+// fixed, file-scope device array instead of memory the library allocates.
+//
+// Who needs it: callers that must not allocate device memory during a
+// match -- code that owns a fixed device-memory budget (or its own pool) and
+// cannot let a library take more, code on a latency-critical path where
+// cudaMalloc/cudaFree's implicit device synchronisation is not acceptable,
+// and code that issues its work into a stream it does not want the library to
+// synchronise with other streams.  They build the data graph's device CCSR
+// once at set-up (gfsm_graph_to_device) and prepare plans on the host; each
+// match then allocates nothing: no cudaMalloc / cudaFree / cudaMallocHost /
+// cudaMallocAsync, no stream or event creation.
+//
+// Limit: the scratch is kNoAllocScratchBytes (64 MiB) per device -- tile
+// status for steps of up to kNoAllocTiles * 1024 candidates plus a frontier
+// arena shared by the query's levels.  Queries always fit because the
+// depth-first chunking shrinks steps to the arena; a query whose plan cannot
+// get even one tile of frontier per level is rejected with
+// GFSM_ERR_TOO_LARGE.  Every process that loads libgfsm.so holds this array
+// on every device where the module is loaded, until it exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoAllocScratchBytes = 64ull << 20;
+constexpr uint32_t kNoAllocTiles = 65536;  // 64M candidates per step
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[kMaxDevices] = {};  // device address of the scratch, per device
+uint32_t g_noalloc_epoch[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfsm_graph *data, void *stream,
+                                                uint64_t *count) {
+    using namespace gfsm;
+    if (!plan || !data || !count) return GFSM_ERR_ARG;
+    if (!data->dev || !data->ctx) return GFSM_ERR_ARG;  // build the device CCSR first (gfsm_graph_to_device)
+    const DeviceGraph &g = *data->dev;
+    const gfsm_limits &lim = data->ctx->lim;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    *count = 0;
+    if (g.device < 0 || g.device >= kMaxDevices) return GFSM_ERR_ARG;
+    if (cudaSetDevice(g.device) != cudaSuccess) return GFSM_ERR_CUDA;
+
+    // The host only knows the array by a stand-in symbol: resolve its device
+    // address once per device, with that device current.  This first call
+    // may load the module, so it belongs before any stream capture.
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    unsigned char *scratch = g_noalloc_ptr[g.device];
+    if (!scratch) {
+        void *addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return GFSM_ERR_CUDA;
+        scratch = static_cast<unsigned char *>(addr);
+        // tile status words must not carry an epoch a later step could reuse
+        if (cudaMemsetAsync(scratch, 0, (uint64_t)kNoAllocTiles * sizeof(TileStatus), st) != cudaSuccess)
+            return GFSM_ERR_CUDA;
+        g_noalloc_ptr[g.device] = scratch;
+        g_noalloc_epoch[g.device] = 0;
+    }
+
+    DQuery dq;
+    uint32_t rlo = 0, rhi = 0;
+    bool never = false;
+    gfsm_status rc = build_dquery(plan->p, g, lim, dq, rlo, rhi, never);
+    if (rc != GFSM_OK) return rc;
+    if (never) return GFSM_OK;
+    const uint32_t dmax = dq.k - 1;
+
+    // scratch layout: tile status | result | counters | tile directory |
+    //                 plan | count | root coff | root slice start | depth buffers
+    unsigned char *p = scratch;
+    TileStatus *status = reinterpret_cast<TileStatus *>(p);
+    p += (uint64_t)kNoAllocTiles * sizeof(TileStatus);
+    StepResult *d_result = reinterpret_cast<StepResult *>(p);
+    p += 256;
+    uint32_t *tile_ctr = reinterpret_cast<uint32_t *>(p);
+    uint32_t *rows_ctr = tile_ctr + 16;
+    p += 256;
+    uint32_t *tile_parent = reinterpret_cast<uint32_t *>(p);
+    p += (((uint64_t)kNoAllocTiles + 2) * 4 + 255) & ~255ull;
+    DQuery *d_plan = reinterpret_cast<DQuery *>(p);
+    p += (sizeof(DQuery) + 255) & ~255ull;
+    unsigned long long *d_count = reinterpret_cast<unsigned long long *>(p);
+    unsigned long long *d_rcoff = d_count + 4;
+    uint32_t *d_rcstart = reinterpret_cast<uint32_t *>(d_count + 8);
+    p += 256;
+    const uint64_t used = (uint64_t)(p - scratch);
+    const uint64_t share = dmax ? ((kNoAllocScratchBytes - used) / dmax) & ~255ull : 0;
+    struct Buf {
+        uint32_t *tup;
+        uint64_t cap;
+        uint32_t *cstart;
+        unsigned long long *coff;
+    } buf[MAXQ];
+    for (uint32_t d = 0; d < dmax; ++d) {
+        const uint64_t per = 4ull * (d + 2) + 4 + 8;
+        uint64_t cap = share > 1024 ? (share - 1024) / per : 0;
+        cap = std::min<uint64_t>(cap, lim.max_soln_size);
+        if (cap < (uint64_t)TILE) return GFSM_ERR_TOO_LARGE;  // needs more than the fixed scratch
+        unsigned char *q = p + share * d;
+        buf[d].cap = cap;
+        buf[d].coff = reinterpret_cast<unsigned long long *>(q);
+        q += ((cap + 1) * 8 + 255) & ~255ull;
+        buf[d].tup = reinterpret_cast<uint32_t *>(q);
+        q += (cap * 4 * (d + 2) + 255) & ~255ull;
+        buf[d].cstart = reinterpret_cast<uint32_t *>(q);
+    }
+
+    // per-call inputs into the scratch; the count must start at zero
+    const unsigned long long rc2[2] = {0ull, (unsigned long long)(rhi - rlo)};
+    if (cudaMemcpyAsync(d_plan, &dq, sizeof(DQuery), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_rcoff, rc2, sizeof(rc2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_rcstart, &rlo, 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(d_count, 0, 8, st) != cudaSuccess || cudaMemsetAsync(rows_ctr, 0, 4, st) != cudaSuccess)
+        return GFSM_ERR_CUDA;
+
+    const uint64_t max_scan = std::min<uint64_t>(lim.max_scan_size, (uint64_t)kNoAllocTiles * TILE);
+    GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
+    unsigned long long total[MAXQ + 1] = {}, pos[MAXQ + 1] = {}, np[MAXQ + 1] = {};
+    double ratio[MAXQ + 1];
+    for (int i = 0; i <= MAXQ; ++i) ratio[i] = 1.0;
+    total[0] = rc2[1];
+    np[0] = 1;
+    uint32_t d = 0;
+    uint32_t &epoch = g_noalloc_epoch[g.device];
+    for (;;) {
+        if (pos[d] >= total[d]) {
+            if (d == 0) break;
+            --d;
+            continue;
+        }
+        const bool emits = d < dmax;
+        unsigned long long chunk = std::min<unsigned long long>(total[d] - pos[d], max_scan);
+        if (emits) {
+            const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
+            chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
+        }
+        const uint32_t ntiles = (uint32_t)div_up(chunk, TILE);
+        if (++epoch >= (1u << 30)) {
+            if (cudaMemsetAsync(status, 0, (uint64_t)kNoAllocTiles * sizeof(TileStatus), st) != cudaSuccess)
+                return GFSM_ERR_CUDA;
+            epoch = 1;
+        }
+        StepArgs a{};
+        a.g = gv;
+        a.plans = d_plan;
+        a.depth = d;
+        if (d == 0) {
+            a.pcstart = d_rcstart;
+            a.pcoff = d_rcoff;
+        } else {
+            a.ptup = buf[d - 1].tup;
+            a.pstride = buf[d - 1].cap;
+            a.pcstart = buf[d - 1].cstart;
+            a.pcoff = buf[d - 1].coff;
+        }
+        a.np = np[d];
+        a.tile_parent = tile_parent;
+        a.c0 = pos[d];
+        a.cend = pos[d] + chunk;
+        a.ntiles = ntiles;
+        if (emits) {
+            a.ctup = buf[d].tup;
+            a.cstride = buf[d].cap;
+            a.ccap = buf[d].cap;
+            a.ccstart = buf[d].cstart;
+            a.ccoff = buf[d].coff;
+        }
+        a.status = status;
+        a.epoch = epoch;
+        a.tile_ctr = tile_ctr;
+        a.counts = d_count;
+        a.result = d_result;
+        a.rows_ctr = rows_ctr;
+        k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(a.pcoff, a.np, a.c0, chunk, ntiles,
+                                                                                 tile_parent, tile_ctr, d_result);
+        if (d == 0) k_step<true><<<ntiles, T, 0, st>>>(a);
+        else k_step<false><<<ntiles, T, 0, st>>>(a);
+        if (cudaGetLastError() != cudaSuccess) return GFSM_ERR_CUDA;
+        StepResult r;
+        if (cudaMemcpyAsync(&r, d_result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return GFSM_ERR_CUDA;
+        if (r.err) return (r.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
+        if (emits && r.n_children > buf[d].cap) {
+            ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
+            continue;
+        }
+        pos[d] += chunk;
+        if (emits) {
+            ratio[d] = std::max(2.0 * (double)r.n_children / (double)chunk, ratio[d] * 0.5);
+            if (r.n_children > 0 && r.total_next > 0) {
+                np[d + 1] = r.n_children;
+                total[d + 1] = r.total_next;
+                pos[d + 1] = 0;
+                ++d;
+            }
+        }
+    }
+    unsigned long long c = 0;
+    if (cudaMemcpyAsync(&c, d_count, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return GFSM_ERR_CUDA;
+    *count = c;
+    return GFSM_OK;
+}

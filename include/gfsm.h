@@ -160,6 +160,23 @@ gfsm_status gfsm_match_count(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_gr
 gfsm_status gfsm_match_mappings(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data,
                                 uint32_t *rows, uint64_t max_rows, uint64_t *n_rows,
                                 uint64_t *count, gfsm_stats *stats);
+/* No counterpart in the reference.  Counts one query like gfsm_match_count
+ * but allocates no device memory: no cudaMalloc / cudaFree / cudaMallocHost /
+ * cudaMallocAsync and no stream or event creation.  It is meant for callers
+ * that may not allocate during a match -- a fixed device-memory budget or
+ * pool, a latency-critical path that cannot take cudaMalloc/cudaFree's
+ * implicit synchronisation.  All scratch lives in one fixed 64 MiB device
+ * array inside libgfsm.so (held on each device that loads the library until
+ * the process exits); data's device CCSR must already exist
+ * (gfsm_graph_to_device), and the work runs on `stream` (a cudaStream_t,
+ * NULL = the default stream).  The first call on a device resolves the
+ * array's device address and may load the module: make it before any stream
+ * capture.  Every call shares the array, so calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised.  A query
+ * that cannot fit one tile of frontier per level in the array returns
+ * GFSM_ERR_TOO_LARGE. */
+gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfsm_graph *data, void *stream,
+                                     uint64_t *count);
 /* Many queries against one resident data graph in one device pass. */
 gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq,
                              const gfsm_graph *data, uint64_t *counts, gfsm_stats *stats);
