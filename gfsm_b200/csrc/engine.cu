@@ -160,13 +160,58 @@ __device__ __forceinline__ V warp_sum(V x) {
     return x;
 }
 
+// One survivor staged in shared memory between the candidate pass and the
+// coalesced write pass: parent index, candidate, and the child's own
+// next-level candidate slice (start, then its exclusive prefix in the tile).
+struct Stage {
+    uint32_t p, v, cs, cnt;
+};
+
+// First index in a[0, n) with a[i] >= key, searched by a whole warp: 32
+// probes per round narrow the range 32x, so a hub row of 10^5 entries takes
+// four dependent loads instead of seventeen.  All 32 lanes must call it with
+// the same arguments.
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict__ a, uint32_t n, uint32_t key,
+                                                     uint32_t lane) {
+    uint32_t lo = 0, hi = n;  // the answer lies in [lo, hi]
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) >> 5;
+        const uint32_t probe = lo + step * (lane + 1) - 1;  // last index of this lane's segment
+        const bool less = probe < hi && __ldg(a + probe) < key;
+        const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, less));
+        const uint32_t nhi = min(hi, lo + (cnt + 1) * step - 1);
+        lo = lo + cnt * step;
+        hi = nhi;
+    }
+    const bool less = lo + lane < hi && __ldg(a + lo + lane) < key;
+    return lo + __popc(__ballot_sync(0xffffffffu, less));
+}
+
+// Branch-free lower bound over a shared-memory array.
+__device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t n, uint32_t key) {
+    if (n == 0) return 0;
+    const uint32_t *base = a;
+    while (n > 1) {
+        const uint32_t half = n >> 1;
+        base = (base[half] < key) ? base + half : base;
+        n -= half;
+    }
+    return (uint32_t)(base - a) + (*base < key ? 1u : 0u);
+}
+
+constexpr int WC = 32 * CPT;        // candidates per warp per tile (a contiguous run)
+constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
+constexpr int REQ_SMEM = 1024;      // entries staged per requirement row
+
 template <bool ROOT>
-__global__ void __launch_bounds__(T) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(T, 4) k_step(const StepArgs a) {
     __shared__ unsigned long long s_coff[WIN];
-    __shared__ uint32_t s_wcnt[CPT][NWARP];
-    __shared__ unsigned long long s_wdeg[CPT][NWARP];
-    __shared__ unsigned long long s_wbytes[NWARP];
-    __shared__ uint32_t s_tile, s_q0;
+    __shared__ Stage s_stage[TILE];
+    __shared__ uint32_t s_req[NSTAGE][REQ_SMEM];
+    __shared__ uint32_t s_rlo[NSTAGE], s_rhi[NSTAGE], s_rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
+    __shared__ uint32_t s_wcnt[NWARP], s_wofs[NWARP + 1];
+    __shared__ unsigned long long s_wdeg[NWARP], s_wdofs[NWARP], s_wbytes[NWARP];
+    __shared__ uint32_t s_tile, s_q0, s_vfirst, s_vlast;
     __shared__ unsigned long long s_excl_cnt, s_excl_deg, s_agg_cnt, s_agg_deg, s_fcount;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -174,115 +219,169 @@ __global__ void __launch_bounds__(T) k_step(const StepArgs a) {
         s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
         s_fcount = 0;
     }
+    if (tid < NSTAGE) s_rmode[tid] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const unsigned long long base = a.c0 + (unsigned long long)tile * TILE;
+    const unsigned long long tend = min(base + (unsigned long long)TILE, a.cend);
     const uint32_t plo = a.tile_parent[tile], phi = a.tile_parent[tile + 1];
     const uint32_t nwin = phi - plo + 2;  // coff[plo .. phi+1]
     const bool win_smem = nwin <= (uint32_t)WIN;
     if (win_smem)
         for (uint32_t i = tid; i < nwin; i += T) s_coff[i] = a.pcoff[plo + i];
-    if (tid == 0) s_q0 = ROOT ? plo : a.ptup[plo];
+    const uint32_t d = a.depth;
+    const bool emits = a.ctup != nullptr;
+
+    // ---- a tile inside one parent's slice (hub rows): stage the part of each
+    // requirement row that can hold this tile's candidates
+    const bool single = !ROOT && plo == phi && a.g.elab == nullptr;
+    if (single) {
+        const uint32_t q0 = __ldg(a.ptup + plo);
+        const DLevel *L0 = &a.plans[q0].lv[d];
+        if (tid == 0) {
+            const uint32_t cs0 = __ldg(a.pcstart + plo);
+            const unsigned long long c00 = a.pcoff[plo];
+            s_vfirst = __ldg(a.g.adj + cs0 + (uint32_t)(base - c00));
+            s_vlast = __ldg(a.g.adj + cs0 + (uint32_t)(tend - 1 - c00));
+        }
+        __syncthreads();
+        if (warp < 2 * NSTAGE) {
+            const uint32_t r = warp >> 1;
+            if (r < L0->nreq && L0->req_pos[r] != REQ_SELF) {
+                const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + L0->req_pos[r]) * a.pstride + plo);
+                const uint32_t rs = __ldg(a.g.rowptr + u), re = __ldg(a.g.rowptr + u + 1);
+                const uint32_t key = (warp & 1) ? s_vlast + 1 : s_vfirst;
+                const uint32_t b = rs + warp_lower_bound(a.g.adj + rs, re - rs, key, lane);
+                if (lane == 0) {
+                    if (warp & 1) s_rhi[r] = b; else s_rlo[r] = b;
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t r = 0; r < (uint32_t)NSTAGE; ++r) {
+            if (r >= L0->nreq || L0->req_pos[r] == REQ_SELF) continue;
+            const uint32_t lo = s_rlo[r], n = s_rhi[r] - s_rlo[r];
+            if (n <= (uint32_t)REQ_SMEM)
+                for (uint32_t i = tid; i < n; i += T) s_req[r][i] = __ldg(a.g.adj + lo + i);
+            if (tid == 0) s_rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
+        }
+    }
+    if (tid == 0) s_q0 = ROOT ? plo : __ldg(a.ptup + plo);
     __syncthreads();
 
-    const uint32_t d = a.depth;
-    uint32_t cpar[CPT], cv[CPT], cst[CPT], ccnt[CPT];
-    bool cemit[CPT];
-    unsigned long long my_bytes = 0;
-    uint32_t fq = 0xffffffffu;
-    unsigned long long fc = 0;
+    unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
+    uint32_t fq = 0xffffffffu, wcnt = 0;
+    Stage *wstage = s_stage + warp * WC;
 
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < CPT; ++j) {
-        cemit[j] = false;
-        cpar[j] = 0; cv[j] = 0; cst[j] = 0; ccnt[j] = 0;
-        const unsigned long long c = base + (unsigned long long)(j * T) + tid;
-        if (c >= a.cend) continue;
-        // parent = largest p in [plo, phi] with coff[p] <= c
-        uint32_t lo = 0, hi = nwin - 1;
-        if (win_smem) {
-            while (hi - lo > 1) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (s_coff[mid] <= c) lo = mid; else hi = mid;
+        const unsigned long long c = base + (unsigned long long)(warp * WC + j * 32) + lane;
+        bool emit = false;
+        Stage rec{0, 0, 0, 0};
+        if (c < tend) {
+            // parent = largest p in [plo, phi] with coff[p] <= c
+            uint32_t lo = 0, hi = nwin - 1;
+            if (win_smem) {
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (s_coff[mid] <= c) lo = mid; else hi = mid;
+                }
+            } else {
+                while (hi - lo > 1) {
+                    const uint32_t mid = lo + ((hi - lo) >> 1);
+                    if (a.pcoff[plo + mid] <= c) lo = mid; else hi = mid;
+                }
             }
-        } else {
-            while (hi - lo > 1) {
-                uint32_t mid = lo + ((hi - lo) >> 1);
-                if (a.pcoff[plo + mid] <= c) lo = mid; else hi = mid;
+            const uint32_t p = plo + lo;
+            const unsigned long long pc = win_smem ? s_coff[lo] : a.pcoff[p];
+            const uint32_t local = (uint32_t)(c - pc);
+            const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
+            const DLevel *L = &a.plans[q].lv[d];
+            uint32_t v;
+            bool pass = true;
+            if (ROOT) {
+                v = __ldg(a.pcstart + p) + local;
+                my_bytes += 4;  // degree/label read of a data vertex
+            } else {
+                const uint32_t idx = __ldg(a.pcstart + p) + local;
+                v = __ldg(a.g.adj + idx);
+                const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
+                if (L->anchor_check) pass = has_edge(a.g, anchor, v, L->anchor_lab);
+                else if (a.g.elab) pass = __ldg(a.g.elab + idx) == L->anchor_lab;
+                // injectivity (HnGPU.cu:223-236)
+                for (uint32_t i = 0; i < d; ++i)
+                    if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+                if (local == 0) {
+                    // algorithmic bytes of this parent: its tuple and every backward
+                    // neighbour's row (anchor + requirement rows), read once
+                    unsigned long long b = 4ull * d;
+                    b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
+                    for (uint32_t r = 0; r < L->nreq; ++r) {
+                        const uint32_t pos = L->req_pos[r];
+                        if (pos == REQ_SELF) continue;
+                        const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                        b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
+                    }
+                    my_bytes += b;
+                }
             }
-        }
-        const uint32_t p = plo + lo;
-        const unsigned long long pc = win_smem ? s_coff[lo] : a.pcoff[p];
-        const uint32_t local = (uint32_t)(c - pc);
-        const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
-        const DLevel *L = &a.plans[q].lv[d];
-        uint32_t v;
-        bool pass = true;
-        if (ROOT) {
-            v = __ldg(a.pcstart + p) + local;
-            my_bytes += 4;  // degree/label read of a data vertex
-        } else {
-            const uint32_t idx = __ldg(a.pcstart + p) + local;
-            v = __ldg(a.g.adj + idx);
-            const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
-            if (L->anchor_check) pass = has_edge(a.g, anchor, v, L->anchor_lab);
-            else if (a.g.elab) pass = __ldg(a.g.elab + idx) == L->anchor_lab;
-            // injectivity (HnGPU.cu:223-236)
-#pragma unroll
-            for (int i = 0; i < MAXQ; ++i)
-                if ((uint32_t)i < d && __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
-            if (local == 0) {
-                // algorithmic bytes of this parent: its tuple and every backward
-                // neighbour's row (anchor + requirement rows), read once
-                unsigned long long b = 4ull * d;
-                b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
-                for (uint32_t r = 0; r < L->nreq; ++r) {
+            // remaining requirements (HnGPU.cu:243-252)
+            for (uint32_t r = 0; r < L->nreq && pass; ++r) {
+                const uint32_t mode = (single && r < (uint32_t)NSTAGE) ? s_rmode[r] : 0u;
+                if (mode == 1u) {
+                    const uint32_t n = s_rhi[r] - s_rlo[r];
+                    const uint32_t k = smem_lower_bound(s_req[r], n, v);
+                    pass = k < n && s_req[r][k] == v && L->req_lab[r] == a.g.single_label;
+                } else if (mode == 2u) {
+                    const uint32_t n = s_rhi[r] - s_rlo[r];
+                    const uint32_t k = lower_bound_u32(a.g.adj + s_rlo[r], n, v);
+                    pass = k < n && __ldg(a.g.adj + s_rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
+                } else {
                     const uint32_t pos = L->req_pos[r];
-                    if (pos == REQ_SELF) continue;
-                    const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                    b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
-                }
-                my_bytes += b;
-            }
-        }
-        // remaining requirements (HnGPU.cu:243-252)
-        for (uint32_t r = 0; r < L->nreq && pass; ++r) {
-            const uint32_t pos = L->req_pos[r];
-            const uint32_t u = pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-            pass = has_edge(a.g, u, v, L->req_lab[r]);
-        }
-        if (!pass) continue;
-        if (L->final_) {
-            if (a.rows_out) {
-                const uint32_t slot = atomicAdd(a.rows_ctr, 1u);
-                if (slot < a.max_rows) {
-                    const DQuery *Q = &a.plans[q];
-                    uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
-                    for (uint32_t i = 0; i < d; ++i)
-                        row[Q->col[i]] = __ldg(a.g.order + __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
-                    row[Q->col[d]] = __ldg(a.g.order + v);
+                    const uint32_t u =
+                        pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                    pass = has_edge(a.g, u, v, L->req_lab[r]);
                 }
             }
-            if (fc && q != fq) {
-                atomicAdd(&a.counts[fq], fc);
-                fc = 0;
+            if (pass) {
+                if (L->final_) {
+                    if (a.rows_out) {
+                        const uint32_t slot = atomicAdd(a.rows_ctr, 1u);
+                        if (slot < a.max_rows) {
+                            const DQuery *Q = &a.plans[q];
+                            uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
+                            for (uint32_t i = 0; i < d; ++i)
+                                row[Q->col[i]] =
+                                    __ldg(a.g.order + __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
+                            row[Q->col[d]] = __ldg(a.g.order + v);
+                        }
+                    }
+                    if (fc && q != fq) {
+                        atomicAdd(&a.counts[fq], fc);
+                        fc = 0;
+                    }
+                    fq = q;
+                    ++fc;
+                } else {
+                    // the child's own candidate slice for depth+1
+                    const uint32_t na = L->next_anchor;
+                    const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+                    const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
+                    const uint32_t s = L->next_lo ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo) : rs;
+                    const uint32_t e =
+                        L->next_hi < a.g.n ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi) : re;
+                    if (e > s) {  // a child with no candidates cannot be extended: not written
+                        emit = true;
+                        rec = Stage{p, v, s, e - s};
+                    }
+                }
             }
-            fq = q;
-            ++fc;
-            continue;
         }
-        // the child's own candidate slice for depth+1
-        const uint32_t na = L->next_anchor;
-        const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
-        const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-        const uint32_t s = L->next_lo ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo) : rs;
-        const uint32_t e = L->next_hi < a.g.n ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi) : re;
-        if (e > s) {  // a child with no candidates cannot be extended: not written
-            cemit[j] = true;
-            cpar[j] = p;
-            cv[j] = v;
-            cst[j] = s;
-            ccnt[j] = e - s;
+        if (emits) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, emit);
+            if (emit) wstage[wcnt + __popc(bal & ((1u << lane) - 1u))] = rec;
+            wcnt += __popc(bal);
+            my_deg += emit ? rec.cnt : 0u;
         }
     }
 
@@ -295,34 +394,56 @@ __global__ void __launch_bounds__(T) k_step(const StepArgs a) {
         } else if (fc) {
             atomicAdd(&a.counts[fq], fc);
         }
-    }
-    // ---- rank the children in (j, thread) order
-    {
         const unsigned long long wb = warp_sum(my_bytes);
         if (lane == 0) s_wbytes[warp] = wb;
     }
+    if (!emits) {
+        __syncthreads();
+        if (tid == 0) {
+            unsigned long long bb = 0;
+            for (int w = 0; w < NWARP; ++w) bb += s_wbytes[w];
+            if (bb) atomicAdd(&a.result->alg_bytes, bb);
+            if (s_fcount) atomicAdd(&a.counts[s_q0], s_fcount);
+        }
+        return;
+    }
+    // ---- per-warp exclusive prefix of the staged slice lengths
+    __syncwarp();  // the segment was written by every lane of this warp
+    {
+        const unsigned long long wd = warp_sum(my_deg);
+        // lane l scans entries [4l, 4l+4) of this warp's segment
+        uint32_t loc[CPT];
+        unsigned long long sum = 0;
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-        const uint32_t bal = __ballot_sync(0xffffffffu, cemit[j]);
-        const unsigned long long dg = warp_incl_scan<unsigned long long>(cemit[j] ? ccnt[j] : 0ull, lane);
-        if (lane == 31) {
-            s_wcnt[j][warp] = __popc(bal);
-            s_wdeg[j][warp] = dg;
+        for (int i = 0; i < CPT; ++i) {
+            const uint32_t e = lane * CPT + i;
+            loc[i] = e < wcnt ? wstage[e].cnt : 0u;
+            sum += loc[i];
+        }
+        const unsigned long long incl = warp_incl_scan<unsigned long long>(sum, lane);
+        unsigned long long run = incl - sum;
+#pragma unroll
+        for (int i = 0; i < CPT; ++i) {
+            const uint32_t e = lane * CPT + i;
+            if (e < wcnt) wstage[e].cnt = (uint32_t)run;  // warp-local exclusive prefix (< 2^32)
+            run += loc[i];
+        }
+        if (lane == 0) {
+            s_wcnt[warp] = wcnt;
+            s_wdeg[warp] = wd;
         }
     }
     __syncthreads();
     if (tid == 0) {
         unsigned long long cc = 0, dd = 0, bb = 0;
-        for (int j = 0; j < CPT; ++j)
-            for (int w = 0; w < NWARP; ++w) {
-                const uint32_t x = s_wcnt[j][w];
-                const unsigned long long y = s_wdeg[j][w];
-                s_wcnt[j][w] = (uint32_t)cc;
-                s_wdeg[j][w] = dd;
-                cc += x;
-                dd += y;
-            }
-        for (int w = 0; w < NWARP; ++w) bb += s_wbytes[w];
+        for (int w = 0; w < NWARP; ++w) {
+            s_wofs[w] = (uint32_t)cc;
+            s_wdofs[w] = dd;
+            cc += s_wcnt[w];
+            dd += s_wdeg[w];
+            bb += s_wbytes[w];
+        }
+        s_wofs[NWARP] = (uint32_t)cc;
         s_agg_cnt = cc;
         s_agg_deg = dd;
         if (bb) atomicAdd(&a.result->alg_bytes, bb);
@@ -386,28 +507,27 @@ __global__ void __launch_bounds__(T) k_step(const StepArgs a) {
             if (tile == a.ntiles - 1) {
                 a.result->n_children = ex_cnt + agg_cnt;
                 a.result->total_next = ex_deg + agg_deg;
-                if (ex_cnt + agg_cnt <= a.ccap && a.ccoff) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
+                if (ex_cnt + agg_cnt <= a.ccap) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
             }
         }
     }
     __syncthreads();
-    // ---- write children (SoA: consecutive children -> consecutive words per column)
+    // ---- write the tile's children: consecutive threads -> consecutive slots
     const unsigned long long ex_cnt = s_excl_cnt, ex_deg = s_excl_deg;
-#pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-        const uint32_t bal = __ballot_sync(0xffffffffu, cemit[j]);
-        const unsigned long long dg = warp_incl_scan<unsigned long long>(cemit[j] ? ccnt[j] : 0ull, lane);
-        if (!cemit[j]) continue;
-        const uint64_t slot = ex_cnt + s_wcnt[j][warp] + __popc(bal & ((1u << lane) - 1u));
+    const uint32_t ntot = s_wofs[NWARP];
+    for (uint32_t i = tid; i < ntot; i += T) {
+        uint32_t w = 0;
+        while (w + 1 < (uint32_t)NWARP && s_wofs[w + 1] <= i) ++w;
+        const Stage r = s_stage[w * WC + (i - s_wofs[w])];
+        const uint64_t slot = ex_cnt + i;
         if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
-        const uint32_t p = cpar[j];
-        const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
+        const uint32_t q = ROOT ? r.p : __ldg(a.ptup + r.p);
         a.ctup[slot] = q;
-        for (uint32_t i = 0; i < d; ++i)
-            a.ctup[(uint64_t)(1 + i) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p);
-        a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = cv[j];
-        a.ccstart[slot] = cst[j];
-        a.ccoff[slot] = ex_deg + s_wdeg[j][warp] + dg - ccnt[j];
+        for (uint32_t k = 0; k < d; ++k)
+            a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
+        a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = r.v;
+        a.ccstart[slot] = r.cs;
+        a.ccoff[slot] = ex_deg + s_wdofs[w] + r.cnt;
     }
 }
 
