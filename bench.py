@@ -77,22 +77,33 @@ def barrier(pg):
         pg.barrier()
 
 
+def _device(local):
+    return "cpu" if local is None else f"cuda:{local}"
+
+
 def max_over_ranks(pg, x, local):
+    """Max of x over ranks (local=None reduces on the CPU, for gloo)."""
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([x], dtype=torch.float64, device=_device(local))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
 def sum_over_ranks(pg, x, local):
+    """Sum of x over ranks (local=None reduces on the CPU, for gloo)."""
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([x], dtype=torch.float64, device=_device(local))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
+
+
+def weak_scaling_value(pg, queries_per_rank, seconds, local):
+    """Whole-job queries/s: all ranks' queries over the slowest rank's time."""
+    return sum_over_ranks(pg, float(queries_per_rank), local) / max_over_ranks(pg, seconds, local)
 
 
 def make_workload(rank, nq):
@@ -274,7 +285,7 @@ def run_ours(args, rank, world, local, pg):
     clk = clocks.stop()
     t_dev = max_over_ranks(pg, sum(dev_ms) / 1000.0, local)
     total_queries = sum_over_ranks(pg, float(args.queries * args.steps), local)
-    value = total_queries / t_dev
+    value = weak_scaling_value(pg, args.queries * args.steps, sum(dev_ms) / 1000.0, local)
 
     # -- end to end through the C ABI from host buffers
     barrier(pg)

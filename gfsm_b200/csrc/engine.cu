@@ -80,10 +80,36 @@ struct GraphView {
     uint32_t n;
 };
 
-// reqExists (HnGPU.cu:34-52) as a binary search: does u's row hold (v, lab)?
+// Rows of at most SHORT_ROW entries (most rows of road-like and sparse
+// graphs) are read with independent loads -- one memory round trip -- and
+// searched in registers instead of by a chain of dependent probes.
+constexpr uint32_t SHORT_ROW = 8;
+
+// First index in the row a[0, n) with a[i] >= key, n <= SHORT_ROW.
+__device__ __forceinline__ uint32_t short_lower_bound(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
+    uint32_t r = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < SHORT_ROW; ++i)
+        if (i < n && __ldg(a + i) < key) ++r;
+    return r;
+}
+
+// First index in a[0, n) whose value is >= key, for any n.
+__device__ __forceinline__ uint32_t row_lower_bound(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
+    return n <= SHORT_ROW ? short_lower_bound(a, n, key) : lower_bound_u32(a, n, key);
+}
+
+// reqExists (HnGPU.cu:34-52) as a search: does u's row hold (v, lab)?
 __device__ __forceinline__ bool has_edge(const GraphView &g, uint32_t u, uint32_t v, uint32_t lab) {
     const uint32_t rs = __ldg(g.rowptr + u), re = __ldg(g.rowptr + u + 1);
     if (!g.elab && lab != g.single_label) return false;
+    if (!g.elab && re - rs <= SHORT_ROW) {
+        bool f = false;
+#pragma unroll
+        for (uint32_t i = 0; i < SHORT_ROW; ++i)
+            if (rs + i < re && __ldg(g.adj + rs + i) == v) f = true;
+        return f;
+    }
     uint32_t p = rs + lower_bound_u32(g.adj + rs, re - rs, v);
     if (!g.elab) return p < re && __ldg(g.adj + p) == v;
     for (; p < re && __ldg(g.adj + p) == v; ++p)
@@ -204,7 +230,7 @@ constexpr int NSTAGE = 2;           // requirement rows a single-parent tile sta
 constexpr int REQ_SMEM = 1024;      // entries staged per requirement row
 
 template <bool ROOT>
-__global__ void __launch_bounds__(T, 4) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
     __shared__ unsigned long long s_coff[WIN];
     __shared__ Stage s_stage[TILE];
     __shared__ uint32_t s_req[NSTAGE][REQ_SMEM];
@@ -305,15 +331,17 @@ __global__ void __launch_bounds__(T, 4) k_step(const StepArgs a) {
             } else {
                 const uint32_t idx = __ldg(a.pcstart + p) + local;
                 v = __ldg(a.g.adj + idx);
-                const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
-                if (L->anchor_check) pass = has_edge(a.g, anchor, v, L->anchor_lab);
-                else if (a.g.elab) pass = __ldg(a.g.elab + idx) == L->anchor_lab;
+                if (L->anchor_check)
+                    pass = has_edge(a.g, __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
+                else if (a.g.elab)
+                    pass = __ldg(a.g.elab + idx) == L->anchor_lab;
                 // injectivity (HnGPU.cu:223-236)
                 for (uint32_t i = 0; i < d; ++i)
                     if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
                 if (local == 0) {
                     // algorithmic bytes of this parent: its tuple and every backward
                     // neighbour's row (anchor + requirement rows), read once
+                    const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
                     unsigned long long b = 4ull * d;
                     b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
                     for (uint32_t r = 0; r < L->nreq; ++r) {
@@ -367,9 +395,9 @@ __global__ void __launch_bounds__(T, 4) k_step(const StepArgs a) {
                     const uint32_t na = L->next_anchor;
                     const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
                     const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-                    const uint32_t s = L->next_lo ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo) : rs;
+                    const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
                     const uint32_t e =
-                        L->next_hi < a.g.n ? rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi) : re;
+                        L->next_hi < a.g.n ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_hi) : re;
                     if (e > s) {  // a child with no candidates cannot be extended: not written
                         emit = true;
                         rec = Stage{p, v, s, e - s};

@@ -1,0 +1,119 @@
+"""GPU tests of the served form and of the GFSM command line.
+
+Served form: every request's count is the same alone and in a mix submitted
+concurrently from several host threads across two device slots (their
+batches overlap on the GPU), and the recorded times are ordered.
+
+CLI: the drop-in `GFSM <query> <data>` prints the reference's CSV columns,
+exits with the reference's codes on file errors, and GFSM_OUTPUT=1 writes
+output.fs in the reference's binary layout."""
+import os
+import subprocess
+import threading
+
+import numpy as np
+import pytest
+
+import gfsm_b200
+from gfsm_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+CLI = os.path.join(ROOT, "gfsm_b200", "GFSM")
+
+
+def test_served_alone_equals_in_mix():
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    g = synth.grid(200, 0.05, 0.02, seed=3)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=4)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel).to_device()
+    plans = []
+    for i in range(300):
+        qg, _ = synth.rw_query(g, 3 + i % 7, tree=i % 3 == 0, seed=i)
+        qs, qd = qg.directed()
+        plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    alone = [ctx.match_count(p, data)[0] for p in plans]
+    assert sum(alone) > 0
+    srv = ctx.serve(data, slots=2, max_batch=32)
+
+    def submit(lo, hi):
+        for i in range(lo, hi):
+            srv.submit(plans[i], i)
+
+    ths = [threading.Thread(target=submit, args=(k * 100, (k + 1) * 100)) for k in range(3)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    srv.drain(120000)
+    res = srv.poll(1000)
+    srv.stop()
+    assert len(res) == len(plans)
+    got = {r["req_id"]: r for r in res}
+    for i, c in enumerate(alone):
+        r = got[i]
+        assert r["status"] == 0 and r["count"] == c, (i, r, c)
+        assert r["submit_ms"] <= r["start_ms"] + 1e-6 <= r["done_ms"] + 2e-6
+    ctx.close()
+
+
+def _run(args, env=None, cwd=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([CLI] + args, capture_output=True, text=True, env=e, cwd=cwd, timeout=300)
+
+
+def test_cli_csv_and_count(tmp_path):
+    q = os.path.join(GOLD, "queries", "_4_square.g")
+    d = os.path.join(GOLD, "data", "ba300.g")
+    r = _run([q, d])
+    assert r.returncode == 0, r.stderr
+    line = r.stdout.strip().split("\n")[-1]
+    cols = line.rstrip(",").split(",")
+    # Query,Data,Preallocate,Query Parse,Data Parse,Kernel,Reallocate,ReKernel,Function Count,Solution Write,GPU Time,End to End
+    assert cols[0] == "_4_square.g" and cols[1] == "ba300.g" and len(cols) == 12
+    assert cols[6] == "n/a" and cols[7] == "n/a"
+    oq, od = O.Graph(path=q), O.Graph(path=d)
+    assert int(cols[8]) == O.ffs_count(oq, O.Plan(oq), od, threads=4)
+
+
+def test_cli_exit_codes(tmp_path):
+    q = os.path.join(GOLD, "queries", "_3_triangle.g")
+    assert _run([q, str(tmp_path / "missing.g")]).returncode == 232
+    bad = tmp_path / "bad.g"
+    bad.write_text("t # 1\n1 0 1 1\nt # -1")
+    assert _run([q, str(bad)]).returncode == 233
+    few = tmp_path / "few.g"
+    few.write_text("t # 0\n3 2 1 1\nv 0 1\nt # -1")
+    assert _run([q, str(few)]).returncode == 234
+    disc = tmp_path / "disc.g"
+    disc.write_text("t # 0\n4 4 1 1\nv 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 1 0 1\ne 2 3 1\ne 3 2 1\nt # -1")
+    assert _run([str(disc), os.path.join(GOLD, "data", "er200.g")]).returncode == 1
+
+
+def test_cli_output_fs(tmp_path):
+    q = os.path.join(GOLD, "queries", "_3_triangle.g")
+    d = os.path.join(GOLD, "data", "er200.g")
+    r = _run([q, d], env={"GFSM_OUTPUT": "1"}, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    w = np.fromfile(tmp_path / "output.fs", np.uint32)
+    count, width = int(w[0]), int(w[1])
+    rows = w[2:].reshape(count, width)
+    oq = O.Graph(path=q)
+    od = O.Graph(path=d)
+    qs, qd, ql = oq.edges()
+    ds, dd, dl = od.edges()
+    c2, r2 = O.bt_count(3, qs, qd, ql, None, od.arrays()["count"], ds, dd, dl, None, max_rows=1 << 20)
+    assert count == c2
+    s1 = rows[np.lexsort(rows.T[::-1])]
+    s2 = r2[np.lexsort(r2.T[::-1])]
+    assert np.array_equal(s1, s2)
+    # the soundness predicate of the reference's Java test: every query edge maps to a data edge
+    dset = set(zip(ds.tolist(), dd.tolist()))
+    for row in rows[:5000]:
+        for a, b in zip(qs, qd):
+            assert (int(row[a]), int(row[b])) in dset
