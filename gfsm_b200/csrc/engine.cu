@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -229,32 +230,54 @@ constexpr int WC = 32 * CPT;        // candidates per warp per tile (a contiguou
 constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
 constexpr int REQ_SMEM = 1024;      // entries staged per requirement row
 
-template <bool ROOT>
-__global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
-    __shared__ unsigned long long s_coff[WIN];
-    __shared__ Stage s_stage[TILE];
-    __shared__ uint32_t s_req[NSTAGE][REQ_SMEM];
-    __shared__ uint32_t s_rlo[NSTAGE], s_rhi[NSTAGE], s_rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
-    __shared__ uint32_t s_wcnt[NWARP], s_wofs[NWARP + 1];
-    __shared__ unsigned long long s_wdeg[NWARP], s_wdofs[NWARP], s_wbytes[NWARP];
-    __shared__ uint32_t s_tile, s_q0, s_vfirst, s_vlast;
-    __shared__ unsigned long long s_excl_cnt, s_excl_deg, s_agg_cnt, s_agg_deg, s_fcount;
+// Shared memory of one tile of a level step.
+struct StepSmem {
+    unsigned long long coff[WIN];
+    Stage stage[TILE];
+    uint32_t req[NSTAGE][REQ_SMEM];
+    uint32_t rlo[NSTAGE], rhi[NSTAGE], rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
+    uint32_t wcnt[NWARP], wofs[NWARP + 1];
+    unsigned long long wdeg[NWARP], wdofs[NWARP], wbytes[NWARP];
+    uint32_t q0, vfirst, vlast;
+    unsigned long long excl_cnt, excl_deg, agg_cnt, agg_deg, fcount;
+};
 
+// Loads of frontier data (parent tuples, slice starts, candidate prefixes,
+// the tile directory).  A kernel launch per step may read them through the
+// read-only (non-coherent) path.  The persistent kernel rewrites these
+// buffers within one launch, so it must not: it uses ordinary weak loads,
+// which its grid barrier (release by every writer, acquire by every reader)
+// makes observe the previous step's writes.  The asm keeps the compiler from
+// turning them into read-only-path loads.
+template <bool P>
+__device__ __forceinline__ uint32_t ldf(const uint32_t *p) {
+    if (!P) return __ldg(p);
+    uint32_t v;
+    asm volatile("ld.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+template <bool P>
+__device__ __forceinline__ unsigned long long ldf(const unsigned long long *p) {
+    if (!P) return *p;
+    unsigned long long v;
+    asm volatile("ld.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+
+// One tile of a level step: candidates [c0 + tile*TILE, ...) of the step.
+template <bool ROOT, bool P>
+__device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile, StepSmem &sm) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
-        s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
-        s_fcount = 0;
-    }
-    if (tid < NSTAGE) s_rmode[tid] = 0;
+    if (tid == 0) sm.fcount = 0;
+    if (tid < NSTAGE) sm.rmode[tid] = 0;
     __syncthreads();
-    const uint32_t tile = s_tile;
     const unsigned long long base = a.c0 + (unsigned long long)tile * TILE;
     const unsigned long long tend = min(base + (unsigned long long)TILE, a.cend);
-    const uint32_t plo = a.tile_parent[tile], phi = a.tile_parent[tile + 1];
+    const uint32_t plo = ldf<P>(a.tile_parent + tile), phi = ldf<P>(a.tile_parent + tile + 1);
     const uint32_t nwin = phi - plo + 2;  // coff[plo .. phi+1]
     const bool win_smem = nwin <= (uint32_t)WIN;
     if (win_smem)
-        for (uint32_t i = tid; i < nwin; i += T) s_coff[i] = a.pcoff[plo + i];
+        for (uint32_t i = tid; i < nwin; i += T) sm.coff[i] = ldf<P>(a.pcoff + plo + i);
     const uint32_t d = a.depth;
     const bool emits = a.ctup != nullptr;
 
@@ -262,42 +285,42 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
     // requirement row that can hold this tile's candidates
     const bool single = !ROOT && plo == phi && a.g.elab == nullptr;
     if (single) {
-        const uint32_t q0 = __ldg(a.ptup + plo);
+        const uint32_t q0 = ldf<P>(a.ptup + plo);
         const DLevel *L0 = &a.plans[q0].lv[d];
         if (tid == 0) {
-            const uint32_t cs0 = __ldg(a.pcstart + plo);
-            const unsigned long long c00 = a.pcoff[plo];
-            s_vfirst = __ldg(a.g.adj + cs0 + (uint32_t)(base - c00));
-            s_vlast = __ldg(a.g.adj + cs0 + (uint32_t)(tend - 1 - c00));
+            const uint32_t cs0 = ldf<P>(a.pcstart + plo);
+            const unsigned long long c00 = ldf<P>(a.pcoff + plo);
+            sm.vfirst = __ldg(a.g.adj + cs0 + (uint32_t)(base - c00));
+            sm.vlast = __ldg(a.g.adj + cs0 + (uint32_t)(tend - 1 - c00));
         }
         __syncthreads();
         if (warp < 2 * NSTAGE) {
             const uint32_t r = warp >> 1;
             if (r < L0->nreq && L0->req_pos[r] != REQ_SELF) {
-                const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + L0->req_pos[r]) * a.pstride + plo);
+                const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + L0->req_pos[r]) * a.pstride + plo);
                 const uint32_t rs = __ldg(a.g.rowptr + u), re = __ldg(a.g.rowptr + u + 1);
-                const uint32_t key = (warp & 1) ? s_vlast + 1 : s_vfirst;
+                const uint32_t key = (warp & 1) ? sm.vlast + 1 : sm.vfirst;
                 const uint32_t b = rs + warp_lower_bound(a.g.adj + rs, re - rs, key, lane);
                 if (lane == 0) {
-                    if (warp & 1) s_rhi[r] = b; else s_rlo[r] = b;
+                    if (warp & 1) sm.rhi[r] = b; else sm.rlo[r] = b;
                 }
             }
         }
         __syncthreads();
         for (uint32_t r = 0; r < (uint32_t)NSTAGE; ++r) {
             if (r >= L0->nreq || L0->req_pos[r] == REQ_SELF) continue;
-            const uint32_t lo = s_rlo[r], n = s_rhi[r] - s_rlo[r];
+            const uint32_t lo = sm.rlo[r], n = sm.rhi[r] - sm.rlo[r];
             if (n <= (uint32_t)REQ_SMEM)
-                for (uint32_t i = tid; i < n; i += T) s_req[r][i] = __ldg(a.g.adj + lo + i);
-            if (tid == 0) s_rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
+                for (uint32_t i = tid; i < n; i += T) sm.req[r][i] = __ldg(a.g.adj + lo + i);
+            if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
         }
     }
-    if (tid == 0) s_q0 = ROOT ? plo : __ldg(a.ptup + plo);
+    if (tid == 0) sm.q0 = ROOT ? plo : ldf<P>(a.ptup + plo);
     __syncthreads();
 
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
     uint32_t fq = 0xffffffffu, wcnt = 0;
-    Stage *wstage = s_stage + warp * WC;
+    Stage *wstage = sm.stage + warp * WC;
 
 #pragma unroll 1
     for (int j = 0; j < CPT; ++j) {
@@ -310,44 +333,44 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
             if (win_smem) {
                 while (hi - lo > 1) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (s_coff[mid] <= c) lo = mid; else hi = mid;
+                    if (sm.coff[mid] <= c) lo = mid; else hi = mid;
                 }
             } else {
                 while (hi - lo > 1) {
                     const uint32_t mid = lo + ((hi - lo) >> 1);
-                    if (a.pcoff[plo + mid] <= c) lo = mid; else hi = mid;
+                    if (ldf<P>(a.pcoff + plo + mid) <= c) lo = mid; else hi = mid;
                 }
             }
             const uint32_t p = plo + lo;
-            const unsigned long long pc = win_smem ? s_coff[lo] : a.pcoff[p];
+            const unsigned long long pc = win_smem ? sm.coff[lo] : ldf<P>(a.pcoff + p);
             const uint32_t local = (uint32_t)(c - pc);
-            const uint32_t q = ROOT ? p : __ldg(a.ptup + p);
+            const uint32_t q = ROOT ? p : ldf<P>(a.ptup + p);
             const DLevel *L = &a.plans[q].lv[d];
             uint32_t v;
             bool pass = true;
             if (ROOT) {
-                v = __ldg(a.pcstart + p) + local;
+                v = ldf<P>(a.pcstart + p) + local;
                 my_bytes += 4;  // degree/label read of a data vertex
             } else {
-                const uint32_t idx = __ldg(a.pcstart + p) + local;
+                const uint32_t idx = ldf<P>(a.pcstart + p) + local;
                 v = __ldg(a.g.adj + idx);
                 if (L->anchor_check)
-                    pass = has_edge(a.g, __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
+                    pass = has_edge(a.g, ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
                 else if (a.g.elab)
                     pass = __ldg(a.g.elab + idx) == L->anchor_lab;
                 // injectivity (HnGPU.cu:223-236)
                 for (uint32_t i = 0; i < d; ++i)
-                    if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+                    if (ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
                 if (local == 0) {
                     // algorithmic bytes of this parent: its tuple and every backward
                     // neighbour's row (anchor + requirement rows), read once
-                    const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
+                    const uint32_t anchor = ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
                     unsigned long long b = 4ull * d;
                     b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
                     for (uint32_t r = 0; r < L->nreq; ++r) {
                         const uint32_t pos = L->req_pos[r];
                         if (pos == REQ_SELF) continue;
-                        const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                        const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
                         b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
                     }
                     my_bytes += b;
@@ -355,19 +378,19 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
             }
             // remaining requirements (HnGPU.cu:243-252)
             for (uint32_t r = 0; r < L->nreq && pass; ++r) {
-                const uint32_t mode = (single && r < (uint32_t)NSTAGE) ? s_rmode[r] : 0u;
+                const uint32_t mode = (single && r < (uint32_t)NSTAGE) ? sm.rmode[r] : 0u;
                 if (mode == 1u) {
-                    const uint32_t n = s_rhi[r] - s_rlo[r];
-                    const uint32_t k = smem_lower_bound(s_req[r], n, v);
-                    pass = k < n && s_req[r][k] == v && L->req_lab[r] == a.g.single_label;
+                    const uint32_t n = sm.rhi[r] - sm.rlo[r];
+                    const uint32_t k = smem_lower_bound(sm.req[r], n, v);
+                    pass = k < n && sm.req[r][k] == v && L->req_lab[r] == a.g.single_label;
                 } else if (mode == 2u) {
-                    const uint32_t n = s_rhi[r] - s_rlo[r];
-                    const uint32_t k = lower_bound_u32(a.g.adj + s_rlo[r], n, v);
-                    pass = k < n && __ldg(a.g.adj + s_rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
+                    const uint32_t n = sm.rhi[r] - sm.rlo[r];
+                    const uint32_t k = lower_bound_u32(a.g.adj + sm.rlo[r], n, v);
+                    pass = k < n && __ldg(a.g.adj + sm.rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
                 } else {
                     const uint32_t pos = L->req_pos[r];
                     const uint32_t u =
-                        pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                        pos == REQ_SELF ? v : ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
                     pass = has_edge(a.g, u, v, L->req_lab[r]);
                 }
             }
@@ -380,7 +403,7 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
                             uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
                             for (uint32_t i = 0; i < d; ++i)
                                 row[Q->col[i]] =
-                                    __ldg(a.g.order + __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
+                                    __ldg(a.g.order + ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
                             row[Q->col[d]] = __ldg(a.g.order + v);
                         }
                     }
@@ -393,7 +416,7 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
                 } else {
                     // the child's own candidate slice for depth+1
                     const uint32_t na = L->next_anchor;
-                    const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+                    const uint32_t w = na == d ? v : ldf<P>(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
                     const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
                     const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
                     const uint32_t e =
@@ -415,23 +438,23 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
 
     // ---- final-depth counts: one shared add per warp in the common case
     {
-        const bool uniform = __all_sync(0xffffffffu, fc == 0 || fq == s_q0);
+        const bool uniform = __all_sync(0xffffffffu, fc == 0 || fq == sm.q0);
         if (uniform) {
             const unsigned long long sum = warp_sum(fc);
-            if (lane == 0 && sum) atomicAdd(&s_fcount, sum);
+            if (lane == 0 && sum) atomicAdd(&sm.fcount, sum);
         } else if (fc) {
             atomicAdd(&a.counts[fq], fc);
         }
         const unsigned long long wb = warp_sum(my_bytes);
-        if (lane == 0) s_wbytes[warp] = wb;
+        if (lane == 0) sm.wbytes[warp] = wb;
     }
     if (!emits) {
         __syncthreads();
         if (tid == 0) {
             unsigned long long bb = 0;
-            for (int w = 0; w < NWARP; ++w) bb += s_wbytes[w];
+            for (int w = 0; w < NWARP; ++w) bb += sm.wbytes[w];
             if (bb) atomicAdd(&a.result->alg_bytes, bb);
-            if (s_fcount) atomicAdd(&a.counts[s_q0], s_fcount);
+            if (sm.fcount) atomicAdd(&a.counts[sm.q0], sm.fcount);
         }
         return;
     }
@@ -457,31 +480,31 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
             run += loc[i];
         }
         if (lane == 0) {
-            s_wcnt[warp] = wcnt;
-            s_wdeg[warp] = wd;
+            sm.wcnt[warp] = wcnt;
+            sm.wdeg[warp] = wd;
         }
     }
     __syncthreads();
     if (tid == 0) {
         unsigned long long cc = 0, dd = 0, bb = 0;
         for (int w = 0; w < NWARP; ++w) {
-            s_wofs[w] = (uint32_t)cc;
-            s_wdofs[w] = dd;
-            cc += s_wcnt[w];
-            dd += s_wdeg[w];
-            bb += s_wbytes[w];
+            sm.wofs[w] = (uint32_t)cc;
+            sm.wdofs[w] = dd;
+            cc += sm.wcnt[w];
+            dd += sm.wdeg[w];
+            bb += sm.wbytes[w];
         }
-        s_wofs[NWARP] = (uint32_t)cc;
-        s_agg_cnt = cc;
-        s_agg_deg = dd;
+        sm.wofs[NWARP] = (uint32_t)cc;
+        sm.agg_cnt = cc;
+        sm.agg_deg = dd;
         if (bb) atomicAdd(&a.result->alg_bytes, bb);
-        if (s_fcount) atomicAdd(&a.counts[s_q0], s_fcount);
+        if (sm.fcount) atomicAdd(&a.counts[sm.q0], sm.fcount);
     }
     __syncthreads();
     // ---- decoupled look-back (warp 0)
     if (warp == 0) {
-        const uint32_t agg_cnt = (uint32_t)s_agg_cnt;
-        const unsigned long long agg_deg = s_agg_deg;
+        const uint32_t agg_cnt = (uint32_t)sm.agg_cnt;
+        const unsigned long long agg_deg = sm.agg_deg;
         unsigned long long ex_cnt = 0, ex_deg = 0;
         TileStatus *st = a.status;
         if (tile == 0) {
@@ -530,8 +553,8 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
             }
         }
         if (lane == 0) {
-            s_excl_cnt = ex_cnt;
-            s_excl_deg = ex_deg;
+            sm.excl_cnt = ex_cnt;
+            sm.excl_deg = ex_deg;
             if (tile == a.ntiles - 1) {
                 a.result->n_children = ex_cnt + agg_cnt;
                 a.result->total_next = ex_deg + agg_deg;
@@ -541,21 +564,204 @@ __global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
     }
     __syncthreads();
     // ---- write the tile's children: consecutive threads -> consecutive slots
-    const unsigned long long ex_cnt = s_excl_cnt, ex_deg = s_excl_deg;
-    const uint32_t ntot = s_wofs[NWARP];
+    const unsigned long long ex_cnt = sm.excl_cnt, ex_deg = sm.excl_deg;
+    const uint32_t ntot = sm.wofs[NWARP];
     for (uint32_t i = tid; i < ntot; i += T) {
         uint32_t w = 0;
-        while (w + 1 < (uint32_t)NWARP && s_wofs[w + 1] <= i) ++w;
-        const Stage r = s_stage[w * WC + (i - s_wofs[w])];
+        while (w + 1 < (uint32_t)NWARP && sm.wofs[w + 1] <= i) ++w;
+        const Stage r = sm.stage[w * WC + (i - sm.wofs[w])];
         const uint64_t slot = ex_cnt + i;
         if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
-        const uint32_t q = ROOT ? r.p : __ldg(a.ptup + r.p);
+        const uint32_t q = ROOT ? r.p : ldf<P>(a.ptup + r.p);
         a.ctup[slot] = q;
         for (uint32_t k = 0; k < d; ++k)
-            a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
+            a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = ldf<P>(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
         a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = r.v;
         a.ccstart[slot] = r.cs;
-        a.ccoff[slot] = ex_deg + s_wdofs[w] + r.cnt;
+        a.ccoff[slot] = ex_deg + sm.wdofs[w] + r.cnt;
+    }
+}
+
+template <bool ROOT>
+__global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
+    __shared__ StepSmem sm;
+    __shared__ uint32_t s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
+    __syncthreads();
+    step_tile<ROOT, false>(a, s_tile, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Device-driven batch: one persistent cooperative launch runs the whole
+// depth-first schedule.  A fixed grid (every CTA resident) takes tiles from
+// a device counter -- the work queue -- and a controller in CTA 0 makes the
+// host loop's decisions (chunk size, retry on overflow, descend / return)
+// between grid barriers, so no step returns to the host.
+// ---------------------------------------------------------------------------
+static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
+
+struct Ctl {
+    unsigned long long total[MAXQ + 1], pos[MAXQ + 1], np[MAXQ + 1];
+    float ratio[MAXQ + 1];
+    uint32_t *tup[MAXQ];
+    unsigned long long cap[MAXQ];
+    uint32_t *cstart[MAXQ];
+    unsigned long long *coff[MAXQ];
+    StepArgs args;               // the step in flight (static fields preset by the host)
+    const unsigned long long *root_coff;
+    const uint32_t *root_cstart;
+    unsigned long long chunk, max_scan, max_candidates;
+    unsigned long long steps, retries, candidates, expansions, alg_bytes;
+    uint32_t d, dmax, emits, done, epoch, err;
+    unsigned int bar_count, bar_gen;
+};
+
+constexpr uint32_t KERR_CAP = 16u;      // max_candidates reached
+
+// Chooses the next step (the host loop's logic); sets done when none is left.
+__device__ void ctl_plan(Ctl &c) {
+    for (;;) {
+        if (c.pos[c.d] < c.total[c.d]) break;
+        if (c.d == 0) {
+            c.done = 1;
+            return;
+        }
+        --c.d;
+    }
+    const uint32_t d = c.d;
+    const bool emits = d < c.dmax;
+    unsigned long long chunk = c.total[d] - c.pos[d];
+    if (chunk > c.max_scan) chunk = c.max_scan;
+    if (emits) {
+        const double allowed = (double)c.cap[d] / fmax((double)c.ratio[d], 1.0 / 8192.0);
+        const unsigned long long lim = (unsigned long long)fmax(allowed, (double)TILE);
+        if (chunk > lim) chunk = lim;
+    }
+    StepArgs &a = c.args;
+    a.depth = d;
+    if (d == 0) {
+        a.ptup = nullptr;
+        a.pstride = 0;
+        a.pcstart = c.root_cstart;
+        a.pcoff = c.root_coff;
+    } else {
+        a.ptup = c.tup[d - 1];
+        a.pstride = c.cap[d - 1];
+        a.pcstart = c.cstart[d - 1];
+        a.pcoff = c.coff[d - 1];
+    }
+    a.np = c.np[d];
+    a.c0 = c.pos[d];
+    a.cend = c.pos[d] + chunk;
+    a.ntiles = (uint32_t)((chunk + TILE - 1) / TILE);
+    if (emits) {
+        a.ctup = c.tup[d];
+        a.cstride = c.cap[d];
+        a.ccap = c.cap[d];
+        a.ccstart = c.cstart[d];
+        a.ccoff = c.coff[d];
+    } else {
+        a.ctup = nullptr;
+        a.cstride = a.ccap = 0;
+        a.ccstart = nullptr;
+        a.ccoff = nullptr;
+    }
+    a.epoch = ++c.epoch;
+    c.chunk = chunk;
+    c.emits = emits;
+    *a.tile_ctr = 0;
+    StepResult *r = a.result;
+    r->n_children = r->total_next = r->alg_bytes = 0;
+    r->err = 0;
+    r->rows = 0;
+}
+
+// Accounts the finished step (the host loop's logic).
+__device__ void ctl_after(Ctl &c) {
+    const StepResult *rp = c.args.result;
+    const unsigned long long n = __ldcg(&rp->n_children), next = __ldcg(&rp->total_next);
+    const unsigned long long ab = __ldcg(&rp->alg_bytes);
+    const uint32_t e = __ldcg(&rp->err);
+    const uint32_t d = c.d;
+    c.steps++;
+    if (e) {
+        c.err |= e;
+        c.done = 1;
+        return;
+    }
+    if (c.emits && n > c.cap[d]) {
+        c.retries++;
+        c.ratio[d] = (float)fmax((double)c.ratio[d] * 4.0, 2.0 * (double)n / (double)c.chunk);
+        return;
+    }
+    c.candidates += c.chunk;
+    c.expansions += n;
+    c.alg_bytes += ab + (c.emits ? n * 4ull * (d + 1) : 0ull);
+    if (c.max_candidates && c.candidates > c.max_candidates) {
+        c.err |= KERR_CAP;
+        c.done = 1;
+        return;
+    }
+    c.pos[d] += c.chunk;
+    if (c.emits) {
+        c.ratio[d] = (float)fmax(2.0 * (double)n / (double)c.chunk, (double)c.ratio[d] * 0.5);
+        if (n > 0 && next > 0) {
+            c.np[d + 1] = n;
+            c.total[d + 1] = next;
+            c.pos[d + 1] = 0;
+            c.d = d + 1;
+        }
+    }
+}
+
+// Per-engine step arguments for the graph-driven schedule: the graph's copy
+// node moves the controller's next StepArgs here, so the step kernels read
+// them from the constant bank like kernel parameters.
+constexpr int kArgSlots = 8;
+__constant__ StepArgs c_args[kArgSlots];
+
+// Graph node: the schedule controller (first: plan the first step; else
+// account the finished step and plan the next) and the loop condition.
+__global__ void k_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int first) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Ctl &c = *ctl;
+    if (first) {
+        ctl_plan(c);
+    } else {
+        ctl_after(c);
+        if (!c.done) ctl_plan(c);
+    }
+    cudaGraphSetConditional(h, c.done ? 0u : 1u);
+}
+
+// Graph node: first parent of every tile of the step (strided fixed grid).
+__global__ void k_part_g(int slot) {
+    const StepArgs &a = c_args[slot];
+    const unsigned long long ncand = a.cend - a.c0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= a.ntiles; t += gridDim.x * blockDim.x) {
+        const unsigned long long c = a.c0 + (t < a.ntiles ? (unsigned long long)t * TILE : ncand - 1);
+        uint64_t lo = 0, hi = a.np;
+        while (hi - lo > 1) {
+            const uint64_t mid = lo + ((hi - lo) >> 1);
+            if (a.pcoff[mid] <= c) lo = mid; else hi = mid;
+        }
+        const_cast<uint32_t *>(a.tile_parent)[t] = (uint32_t)lo;
+    }
+}
+
+// Graph node: the level step on a fixed grid; every CTA takes tiles from the
+// step's counter (in order, so the look-back only waits on running tiles).
+__global__ void __launch_bounds__(T, 6) k_step_g(int slot) {
+    __shared__ StepSmem sm;
+    __shared__ uint32_t s_tile;
+    const StepArgs &a = c_args[slot];
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= a.ntiles) break;
+        if (a.depth == 0) step_tile<true, false>(a, tile, sm);
+        else step_tile<false, false>(a, tile, sm);
     }
 }
 
@@ -657,7 +863,34 @@ gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits 
 
 Engine::~Engine() { release(); }
 
+namespace {
+std::mutex g_slot_mu;
+uint32_t g_slot_used = 0;
+
+int acquire_arg_slot() {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (int i = 0; i < kArgSlots; ++i)
+        if (!(g_slot_used & (1u << i))) {
+            g_slot_used |= 1u << i;
+            return i;
+        }
+    return -1;
+}
+
+void release_arg_slot(int s) {
+    if (s < 0) return;
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    g_slot_used &= ~(1u << s);
+}
+}  // namespace
+
 void Engine::release() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    release_arg_slot(arg_slot);
+    arg_slot = -1;
     if (arena) cudaFree(arena);
     if (small) cudaFree(small);
     if (h_result) cudaFreeHost(h_result);
@@ -685,7 +918,8 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
     status_tiles = (uint32_t)div_up(max_scan, TILE);
     // small region: tile status, tile directory, counters, result, plans
-    small_bytes = (uint64_t)status_tiles * sizeof(TileStatus) + ((uint64_t)status_tiles + 2) * 4 + 512;
+    small_bytes = (uint64_t)status_tiles * sizeof(TileStatus) + ((((uint64_t)status_tiles + 2) * 4 + 255) & ~255ull) +
+                  512 + ((sizeof(Ctl) + 255) & ~255ull);
     ECHECK(cudaMalloc(&small, small_bytes));
     ECHECK(cudaMemsetAsync(small, 0, small_bytes, stream));
     char *p = static_cast<char *>(small);
@@ -698,8 +932,17 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     rows_ctr = reinterpret_cast<uint32_t *>(p);
     p += 64;
     tile_parent = reinterpret_cast<uint32_t *>(p);
+    p += (((uint64_t)status_tiles + 2) * 4 + 255) & ~255ull;
+    ctl = p;
     arena_cap = arena_limit;
     epoch = 0;
+    {
+        int sms = 0, per_sm = 0;
+        ECHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_g, T, 0));
+        step_blocks = sms * std::max(per_sm, 1);
+    }
+    arg_slot = acquire_arg_slot();
     ECHECK(cudaStreamSynchronize(stream));
     return GFSM_OK;
 }
@@ -711,6 +954,71 @@ gfsm_status Engine::ensure_arena(uint64_t bytes, std::string &err) {
     arena_bytes = 0;
     ECHECK(cudaMalloc(&arena, bytes));
     arena_bytes = bytes;
+    return GFSM_OK;
+}
+
+// The schedule as a CUDA graph: k_ctl(first) -> WHILE(cond) { copy the step's
+// arguments to this engine's constant slot -> tile directory -> level step ->
+// k_ctl(next step, cond) }.  Every pointer the nodes take is fixed for the
+// engine's lifetime (control block, constant slot), so the graph is built and
+// instantiated once and relaunched by every call.
+gfsm_status Engine::build_graph(std::string &err) {
+    if (graph_exec) return GFSM_OK;
+    if (arg_slot < 0 || graph_failed) return GFSM_ERR_CUDA;
+    cudaGraph_t g = nullptr;
+    auto fail = [&](cudaError_t e, const char *what) {
+        if (g) cudaGraphDestroy(g);
+        graph_failed = true;
+        cudaGetLastError();
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return GFSM_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return fail(e, "cudaGraphCreate");
+    cudaGraphConditionalHandle h;
+    if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
+        return fail(e, "cudaGraphConditionalHandleCreate");
+    Ctl *cp = static_cast<Ctl *>(ctl);
+    int first = 1, next = 0, slot = arg_slot;
+    void *a_first[] = {&cp, &h, &first};
+    void *a_next[] = {&cp, &h, &next};
+    void *a_slot[] = {&slot};
+    cudaKernelNodeParams kp{};
+    kp.func = (void *)k_ctl;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = a_first;
+    cudaGraphNode_t n0, n1;
+    if ((e = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp)) != cudaSuccess) return fail(e, "ctl node");
+    cudaGraphNodeParams cnp{};
+    cnp.type = cudaGraphNodeTypeConditional;
+    cnp.conditional.handle = h;
+    cnp.conditional.type = cudaGraphCondTypeWhile;
+    cnp.conditional.size = 1;
+    if ((e = cudaGraphAddNode(&n1, g, &n0, 1, &cnp)) != cudaSuccess) return fail(e, "while node");
+    cudaGraph_t body = cnp.conditional.phGraph_out[0];
+    cudaGraphNode_t b0, b1, b2, b3;
+    if ((e = cudaGraphAddMemcpyNodeToSymbol(&b0, body, nullptr, 0, c_args, &cp->args, sizeof(StepArgs),
+                                            (size_t)slot * sizeof(StepArgs), cudaMemcpyDeviceToDevice)) != cudaSuccess)
+        return fail(e, "args copy node");
+    kp.func = (void *)k_part_g;
+    kp.gridDim = dim3((unsigned)step_blocks);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = a_slot;
+    if ((e = cudaGraphAddKernelNode(&b1, body, &b0, 1, &kp)) != cudaSuccess) return fail(e, "partition node");
+    kp.func = (void *)k_step_g;
+    kp.blockDim = dim3(T);
+    if ((e = cudaGraphAddKernelNode(&b2, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "step node");
+    kp.func = (void *)k_ctl;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = a_next;
+    if ((e = cudaGraphAddKernelNode(&b3, body, &b2, 1, &kp)) != cudaSuccess) return fail(e, "ctl node");
+    if ((e = cudaGraphInstantiate(&graph_exec, g, 0)) != cudaSuccess) {
+        graph_exec = nullptr;
+        return fail(e, "cudaGraphInstantiate");
+    }
+    graph = g;
     return GFSM_OK;
 }
 
@@ -820,6 +1128,92 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
 
     GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
+    // GFSM_TRACE=1: one line per step on stderr (depth, candidates, survivors,
+    // kernel ms) -- the per-level frontier statistics of the reference's
+    // pcsv_printf HnStep / HnPred lines (HnGPU.cu:431, 525)
+    static const bool trace = [] {
+        const char *t = getenv("GFSM_TRACE");
+        return t && *t && *t != '0';
+    }();
+    // GFSM_DRIVER=graph runs the whole schedule as one CUDA graph launch; the
+    // default host-driven loop launches each step and reads its totals back.
+    const char *drv = getenv("GFSM_DRIVER");
+    const bool graph_driver = !trace && drv && !strcmp(drv, "graph") && build_graph(err) == GFSM_OK;
+    if (graph_driver) {
+        if (epoch > (1u << 30) - (1u << 24)) {
+            ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));
+            epoch = 0;
+        }
+        Ctl c;
+        std::memset(&c, 0, sizeof(c));
+        c.total[0] = rcoff[na];
+        c.np[0] = na;
+        for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = 1.0f;
+        for (uint32_t i = 0; i < dmax; ++i) {
+            c.tup[i] = buf[i].tup;
+            c.cap[i] = buf[i].cap;
+            c.cstart[i] = buf[i].cstart;
+            c.coff[i] = buf[i].coff;
+        }
+        c.root_coff = d_rcoff;
+        c.root_cstart = d_rcstart;
+        c.max_scan = max_scan;
+        c.max_candidates = lim.max_candidates;
+        c.dmax = dmax;
+        c.epoch = epoch;
+        StepArgs &a = c.args;
+        a.g = gv;
+        a.plans = d_plans;
+        a.tile_parent = tile_parent;
+        a.status = status;
+        a.tile_ctr = tile_ctr;
+        a.counts = d_counts;
+        a.result = d_result;
+        a.rows_out = d_rows;
+        a.max_rows = max_rows;
+        a.rows_ctr = rows_ctr;
+        Ctl *d_ctl = static_cast<Ctl *>(ctl);
+        ECHECK(cudaMemcpyAsync(d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+        st.h2d_bytes += sizeof(Ctl);
+        ECHECK(cudaEventRecord(ev0, stream));
+        ECHECK(cudaGraphLaunch(graph_exec, stream));
+        ECHECK(cudaEventRecord(ev1, stream));
+        ECHECK(cudaMemcpyAsync(&c, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+        std::vector<unsigned long long> cnt(na);
+        ECHECK(cudaMemcpyAsync(cnt.data(), d_counts, (uint64_t)na * 8, cudaMemcpyDeviceToHost, stream));
+        ECHECK(cudaStreamSynchronize(stream));
+        st.d2h_bytes += sizeof(Ctl) + (uint64_t)na * 8;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        epoch = c.epoch;
+        st.steps = c.steps;
+        st.retries = c.retries;
+        st.candidates = c.candidates;
+        st.expansions = c.expansions;
+        st.alg_bytes = c.alg_bytes;
+        st.kernel_ms = ms;
+        st.device_ms = ms;
+        if (c.err) {
+            err = "device schedule error bits " + std::to_string(c.err);
+            if (stats) *stats = st;
+            if (c.err & KERR_CAP) return GFSM_ERR_TOO_LARGE;
+            return (c.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
+        }
+        for (uint32_t i = 0; i < na; ++i) counts_out[active[i]] = cnt[i];
+        if (rows_out) {
+            uint32_t claimed = 0;
+            ECHECK(cudaMemcpy(&claimed, rows_ctr, 4, cudaMemcpyDeviceToHost));
+            const uint64_t nr = std::min<uint64_t>(claimed, max_rows);
+            if (nr) ECHECK(cudaMemcpy(rows_out, d_rows, nr * dq[0].k * 4, cudaMemcpyDeviceToHost));
+            st.d2h_bytes += nr * dq[0].k * 4;
+            if (n_rows) *n_rows = nr;
+        }
+        for (uint32_t i = 0; i < na; ++i) st.count += cnt[i];
+        st.wall_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        if (stats) *stats = st;
+        return GFSM_OK;
+    }
     std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0);
     std::vector<double> ratio(dmax + 1, 1.0);
     total[0] = rcoff[na];
@@ -903,6 +1297,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
             continue;
         }
+        if (trace)
+            fprintf(stderr, "gfsm-step depth=%u cand=%llu children=%llu next=%llu tiles=%u ms=%.4f\n", d, chunk,
+                    emits ? r.n_children : 0ull, emits ? r.total_next : 0ull, ntiles, ms);
         st.candidates += chunk;
         st.expansions += r.n_children;
         if (lim.max_candidates && st.candidates > lim.max_candidates) {

@@ -27,6 +27,13 @@ struct Engine {
     uint32_t *tile_parent = nullptr;
     uint64_t max_scan = 0;
     uint32_t epoch = 0;
+    // graph-driven schedule (one graph launch per call; built once per engine)
+    int arg_slot = -1;             // constant-memory slot for this engine's step arguments
+    void *ctl = nullptr;           // device control block (inside the small region)
+    int step_blocks = 0;           // fixed grid of the graph's step kernel
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_failed = false;
 
     Engine() = default;
     Engine(const Engine &) = delete;
@@ -35,6 +42,7 @@ struct Engine {
     void release();
     gfsm_status init(int dev, uint64_t arena_limit, uint64_t scan_limit, std::string &err);
     gfsm_status ensure_arena(uint64_t bytes, std::string &err);
+    gfsm_status build_graph(std::string &err);
     // Counts every plan against g; counts_out[i] for plans[i].  With rows_out
     // (single plan only) also writes up to max_rows full mappings.
     gfsm_status run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,

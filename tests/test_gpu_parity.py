@@ -249,3 +249,32 @@ def test_triangles_medium_rmat(gpu_ctx):
     data = gpu_ctx.graph_from_edges(g.n, s, d)
     tri = gpu_ctx.file_parse(_g("queries/_3_triangle"))
     assert gpu_ctx.solve(tri, data) == 6 * O.triangles(g.n, g.src, g.dst)
+
+
+def test_device_and_host_drivers_agree(monkeypatch):
+    """The graph-driven schedule (one CUDA graph launch, decisions on the
+    device) and the host-driven step loop make the same decisions: identical
+    counts, candidates and expansions."""
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1, mem_limit=256 << 20)
+    g = synth.grid(300, 0.05, 0.02, seed=8)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=9)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
+    plans = []
+    for i in range(40):
+        qg, _ = synth.rw_query(g, 3 + i % 8, tree=i % 2 == 0, seed=50 + i)
+        qs, qd = qg.directed()
+        plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    monkeypatch.setenv("GFSM_DRIVER", "host")
+    host_counts, host_st = ctx.batch_count(plans, data)
+    host_single = [ctx.match_count(p, data) for p in plans[:8]]
+    monkeypatch.setenv("GFSM_DRIVER", "graph")
+    dev_counts, dev_st = ctx.batch_count(plans, data)
+    dev_single = [ctx.match_count(p, data) for p in plans[:8]]
+    assert dev_counts.tolist() == host_counts.tolist()
+    for key in ("candidates", "expansions", "steps", "retries"):
+        assert dev_st[key] == host_st[key], key
+    for (c1, s1), (c2, s2) in zip(host_single, dev_single):
+        assert c1 == c2 and s1["candidates"] == s2["candidates"]
+    assert host_st["steps"] > 20
+    ctx.close()
