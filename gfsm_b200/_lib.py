@@ -86,6 +86,7 @@ class Stats(C.Structure):
         ("wall_ms", C.c_double),
         ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64),
+        ("tile_variant", C.c_int32),
     ]
 
     def as_dict(self):

@@ -29,6 +29,7 @@
 // frontier never exceeds MEMLIMIT (the reference restarts at 2x memory).
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -43,8 +44,6 @@ namespace {
 constexpr int T = 256;
 constexpr int CPT = 4;
 constexpr int TILE = T * CPT;
-constexpr int WIN = TILE + 2;
-constexpr int NWARP = T / 32;
 constexpr uint32_t FLAG_AGG = 1, FLAG_INC = 2;
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
 
@@ -149,10 +148,15 @@ struct StepArgs {
     uint32_t *rows_ctr;
 };
 
+// Also zeroes the step's per-query count scratch: final-level counts of a
+// step are added to the totals only once the host accepts the step, so a step
+// re-run after a frontier overflow never counts twice.
 __global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_t np, unsigned long long c0,
-                            unsigned long long ncand, uint32_t ntiles, uint32_t *__restrict__ tile_parent,
-                            uint32_t *tile_ctr, StepResult *result) {
+                            unsigned long long ncand, uint32_t ntiles, uint32_t tile_size,
+                            uint32_t *__restrict__ tile_parent, uint32_t *tile_ctr, StepResult *result,
+                            unsigned long long *step_counts, uint32_t nq) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t i = t; i < nq; i += gridDim.x * blockDim.x) step_counts[i] = 0;
     if (t == 0) {
         *tile_ctr = 0;
         result->n_children = 0;
@@ -162,13 +166,20 @@ __global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_
         result->rows = 0;
     }
     if (t > ntiles) return;
-    const unsigned long long c = c0 + (t < ntiles ? (unsigned long long)t * TILE : ncand - 1);
+    const unsigned long long c = c0 + (t < ntiles ? (unsigned long long)t * tile_size : ncand - 1);
     uint64_t lo = 0, hi = np;  // largest p with coff[p] <= c
     while (hi - lo > 1) {
         uint64_t mid = lo + ((hi - lo) >> 1);
         if (coff[mid] <= c) lo = mid; else hi = mid;
     }
     tile_parent[t] = (uint32_t)lo;
+}
+
+// Adds an accepted step's final-level counts to the per-query totals.
+__global__ void k_commit(unsigned long long *__restrict__ counts, const unsigned long long *__restrict__ step_counts,
+                         uint32_t nq) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
+        counts[i] += step_counts[i];
 }
 
 template <typename V>
@@ -226,18 +237,35 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
     return (uint32_t)(base - a) + (*base < key ? 1u : 0u);
 }
 
-constexpr int WC = 32 * CPT;        // candidates per warp per tile (a contiguous run)
 constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
 constexpr int REQ_SMEM = 1024;      // entries staged per requirement row
 
+// Tile geometry of a level-step instantiation: threads per CTA, candidates
+// per thread, and the CTAs per SM its register budget is fitted to.
+template <int T_, int CPT_, int MINB_>
+struct Geo {
+    static constexpr int T = T_, CPT = CPT_, TILE = T_ * CPT_, WIN = T_ * CPT_ + 2, NWARP = T_ / 32,
+                         WC = 32 * CPT_, MINB = MINB_;
+};
+using Geo0 = Geo<256, 4, 6>;   // 1024-candidate tiles, 8 warps (the default)
+using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
+using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
+using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
+constexpr int kVariants = 4;
+constexpr uint32_t kMinTile = 512;
+__host__ __device__ constexpr uint32_t variant_tile(int v) {
+    return v == 0 ? Geo0::TILE : v == 1 ? Geo1::TILE : v == 2 ? Geo2::TILE : Geo3::TILE;
+}
+
 // Shared memory of one tile of a level step.
+template <class G>
 struct StepSmem {
-    unsigned long long coff[WIN];
-    Stage stage[TILE];
+    unsigned long long coff[G::WIN];
+    Stage stage[G::TILE];
     uint32_t req[NSTAGE][REQ_SMEM];
     uint32_t rlo[NSTAGE], rhi[NSTAGE], rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
-    uint32_t wcnt[NWARP], wofs[NWARP + 1];
-    unsigned long long wdeg[NWARP], wdofs[NWARP], wbytes[NWARP];
+    uint32_t wcnt[G::NWARP], wofs[G::NWARP + 1];
+    unsigned long long wdeg[G::NWARP], wdofs[G::NWARP], wbytes[G::NWARP];
     uint32_t q0, vfirst, vlast;
     unsigned long long excl_cnt, excl_deg, agg_cnt, agg_deg, fcount;
 };
@@ -265,8 +293,9 @@ __device__ __forceinline__ unsigned long long ldf(const unsigned long long *p) {
 }
 
 // One tile of a level step: candidates [c0 + tile*TILE, ...) of the step.
-template <bool ROOT, bool P>
-__device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile, StepSmem &sm) {
+template <bool ROOT, bool P, class G>
+__device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile, StepSmem<G> &sm) {
+    constexpr int T = G::T, CPT = G::CPT, TILE = G::TILE, WIN = G::WIN, NWARP = G::NWARP, WC = G::WC;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) sm.fcount = 0;
     if (tid < NSTAGE) sm.rmode[tid] = 0;
@@ -582,13 +611,35 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     }
 }
 
-template <bool ROOT>
-__global__ void __launch_bounds__(T, 6) k_step(const StepArgs a) {
-    __shared__ StepSmem sm;
+template <bool ROOT, class G>
+__global__ void __launch_bounds__(G::T, G::MINB) k_step(const StepArgs a) {
+    __shared__ StepSmem<G> sm;
     __shared__ uint32_t s_tile;
     if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
     __syncthreads();
-    step_tile<ROOT, false>(a, s_tile, sm);
+    step_tile<ROOT, false, G>(a, s_tile, sm);
+}
+
+// Launches one level step with the given tile geometry.
+void launch_step(int variant, bool root, const StepArgs &a, uint32_t ntiles, cudaStream_t st) {
+    switch (variant) {
+    case 1:
+        if (root) k_step<true, Geo1><<<ntiles, Geo1::T, 0, st>>>(a);
+        else k_step<false, Geo1><<<ntiles, Geo1::T, 0, st>>>(a);
+        break;
+    case 2:
+        if (root) k_step<true, Geo2><<<ntiles, Geo2::T, 0, st>>>(a);
+        else k_step<false, Geo2><<<ntiles, Geo2::T, 0, st>>>(a);
+        break;
+    case 3:
+        if (root) k_step<true, Geo3><<<ntiles, Geo3::T, 0, st>>>(a);
+        else k_step<false, Geo3><<<ntiles, Geo3::T, 0, st>>>(a);
+        break;
+    default:
+        if (root) k_step<true, Geo0><<<ntiles, Geo0::T, 0, st>>>(a);
+        else k_step<false, Geo0><<<ntiles, Geo0::T, 0, st>>>(a);
+        break;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -610,6 +661,8 @@ struct Ctl {
     StepArgs args;               // the step in flight (static fields preset by the host)
     const unsigned long long *root_coff;
     const uint32_t *root_cstart;
+    unsigned long long *counts;        // per-query totals (args.counts is the step scratch)
+    uint32_t nq, accepted;
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
     uint32_t d, dmax, emits, done, epoch, err;
@@ -684,6 +737,7 @@ __device__ void ctl_after(Ctl &c) {
     const uint32_t e = __ldcg(&rp->err);
     const uint32_t d = c.d;
     c.steps++;
+    c.accepted = 0;
     if (e) {
         c.err |= e;
         c.done = 1;
@@ -694,6 +748,7 @@ __device__ void ctl_after(Ctl &c) {
         c.ratio[d] = (float)fmax((double)c.ratio[d] * 4.0, 2.0 * (double)n / (double)c.chunk);
         return;
     }
+    c.accepted = 1;
     c.candidates += c.chunk;
     c.expansions += n;
     c.alg_bytes += ab + (c.emits ? n * 4ull * (d + 1) : 0ull);
@@ -723,21 +778,30 @@ __constant__ StepArgs c_args[kArgSlots];
 // Graph node: the schedule controller (first: plan the first step; else
 // account the finished step and plan the next) and the loop condition.
 __global__ void k_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int first) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Ctl &c = *ctl;
-    if (first) {
-        ctl_plan(c);
-    } else {
-        ctl_after(c);
-        if (!c.done) ctl_plan(c);
+    __shared__ uint32_t s_accept;
+    if (!first) {
+        if (threadIdx.x == 0) {
+            ctl_after(c);
+            s_accept = c.accepted;
+        }
+        __syncthreads();
+        if (s_accept)  // an accepted step's final-level counts join the totals
+            for (uint32_t i = threadIdx.x; i < c.nq; i += blockDim.x) c.counts[i] += c.args.counts[i];
+        __syncthreads();
     }
-    cudaGraphSetConditional(h, c.done ? 0u : 1u);
+    if (threadIdx.x == 0) {
+        if (first || !c.done) ctl_plan(c);
+        cudaGraphSetConditional(h, c.done ? 0u : 1u);
+    }
 }
 
 // Graph node: first parent of every tile of the step (strided fixed grid).
-__global__ void k_part_g(int slot) {
+__global__ void k_part_g(int slot, const Ctl *ctl) {
     const StepArgs &a = c_args[slot];
     const unsigned long long ncand = a.cend - a.c0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ctl->nq; i += gridDim.x * blockDim.x)
+        a.counts[i] = 0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= a.ntiles; t += gridDim.x * blockDim.x) {
         const unsigned long long c = a.c0 + (t < a.ntiles ? (unsigned long long)t * TILE : ncand - 1);
         uint64_t lo = 0, hi = a.np;
@@ -751,8 +815,8 @@ __global__ void k_part_g(int slot) {
 
 // Graph node: the level step on a fixed grid; every CTA takes tiles from the
 // step's counter (in order, so the look-back only waits on running tiles).
-__global__ void __launch_bounds__(T, 6) k_step_g(int slot) {
-    __shared__ StepSmem sm;
+__global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g(int slot) {
+    __shared__ StepSmem<Geo0> sm;
     __shared__ uint32_t s_tile;
     const StepArgs &a = c_args[slot];
     for (;;) {
@@ -760,8 +824,8 @@ __global__ void __launch_bounds__(T, 6) k_step_g(int slot) {
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= a.ntiles) break;
-        if (a.depth == 0) step_tile<true, false>(a, tile, sm);
-        else step_tile<false, false>(a, tile, sm);
+        if (a.depth == 0) step_tile<true, false, Geo0>(a, tile, sm);
+        else step_tile<false, false, Geo0>(a, tile, sm);
     }
 }
 
@@ -916,7 +980,7 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     ECHECK(cudaEventCreate(&ev_end));
     ECHECK(cudaMallocHost(&h_result, sizeof(StepResult)));
     max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
-    status_tiles = (uint32_t)div_up(max_scan, TILE);
+    status_tiles = (uint32_t)div_up(max_scan, kMinTile);
     // small region: tile status, tile directory, counters, result, plans
     small_bytes = (uint64_t)status_tiles * sizeof(TileStatus) + ((((uint64_t)status_tiles + 2) * 4 + 255) & ~255ull) +
                   512 + ((sizeof(Ctl) + 255) & ~255ull);
@@ -983,10 +1047,11 @@ gfsm_status Engine::build_graph(std::string &err) {
     void *a_first[] = {&cp, &h, &first};
     void *a_next[] = {&cp, &h, &next};
     void *a_slot[] = {&slot};
+    void *a_part[] = {&slot, &cp};
     cudaKernelNodeParams kp{};
     kp.func = (void *)k_ctl;
     kp.gridDim = dim3(1);
-    kp.blockDim = dim3(32);
+    kp.blockDim = dim3(256);
     kp.kernelParams = a_first;
     cudaGraphNode_t n0, n1;
     if ((e = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp)) != cudaSuccess) return fail(e, "ctl node");
@@ -1004,14 +1069,15 @@ gfsm_status Engine::build_graph(std::string &err) {
     kp.func = (void *)k_part_g;
     kp.gridDim = dim3((unsigned)step_blocks);
     kp.blockDim = dim3(256);
-    kp.kernelParams = a_slot;
+    kp.kernelParams = a_part;
     if ((e = cudaGraphAddKernelNode(&b1, body, &b0, 1, &kp)) != cudaSuccess) return fail(e, "partition node");
     kp.func = (void *)k_step_g;
     kp.blockDim = dim3(T);
+    kp.kernelParams = a_slot;
     if ((e = cudaGraphAddKernelNode(&b2, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "step node");
     kp.func = (void *)k_ctl;
     kp.gridDim = dim3(1);
-    kp.blockDim = dim3(32);
+    kp.blockDim = dim3(256);
     kp.kernelParams = a_next;
     if ((e = cudaGraphAddKernelNode(&b3, body, &b2, 1, &kp)) != cudaSuccess) return fail(e, "ctl node");
     if ((e = cudaGraphInstantiate(&graph_exec, g, 0)) != cudaSuccess) {
@@ -1022,9 +1088,48 @@ gfsm_status Engine::build_graph(std::string &err) {
     return GFSM_OK;
 }
 
+// Autotuner: the tile geometry (threads per CTA x candidates per thread) is
+// picked per workload class -- (deepest level, log2 average degree, log2
+// batch size) -- by timing every geometry on a sample of the call's queries
+// the first time a class is seen.  GFSM_TILE=<0..3> forces a geometry and
+// GFSM_AUTOTUNE=0 keeps the default.
+int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
+                         std::string &err) {
+    const char *force = getenv("GFSM_TILE");
+    if (force && *force) {
+        const int v = atoi(force);
+        return v >= 0 && v < kVariants ? v : 0;
+    }
+    const char *at = getenv("GFSM_AUTOTUNE");
+    if (at && *at == '0') return 0;
+    uint32_t kmax = 0;
+    for (const Plan *p : plans) kmax = std::max(kmax, p->k);
+    const double avg = g.n ? (double)g.m / (double)g.n : 0.0;
+    const uint64_t key = ((uint64_t)kmax << 16) | ((uint64_t)std::lround(std::log2(avg + 1.0)) << 8) |
+                         (uint64_t)std::lround(std::log2((double)plans.size() + 1.0));
+    auto it = tuned.find(key);
+    if (it != tuned.end()) return it->second;
+    const size_t ns = std::min<size_t>(plans.size(), 32);
+    std::vector<const Plan *> sample(plans.begin(), plans.begin() + ns);
+    std::vector<uint64_t> cnt(ns);
+    int best = 0;
+    double best_ms = 1e300;
+    for (int v = 0; v < kVariants; ++v) {
+        gfsm_stats s{};
+        if (run(sample, g, lim, cnt.data(), &s, nullptr, 0, nullptr, err, v) != GFSM_OK) return 0;
+        if (s.device_ms < best_ms) {
+            best_ms = s.device_ms;
+            best = v;
+        }
+    }
+    tuned[key] = best;
+    return best;
+}
+
 gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                         uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
-                        uint64_t *n_rows, std::string &err) {
+                        uint64_t *n_rows, std::string &err, int variant) {
+    if (variant < 0) variant = plans.empty() ? 0 : pick_variant(plans, g, lim, err);
     auto t_start = std::chrono::steady_clock::now();
     const int nq = (int)plans.size();
     gfsm_stats st{};
@@ -1063,7 +1168,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
 
     // arena layout: plans | counts | root coff | root cstart | mapping rows | depth buffers
     const uint64_t plans_bytes = (uint64_t)na * sizeof(DQuery);
-    const uint64_t head = ((plans_bytes + 255) & ~255ull) + (((uint64_t)na * 8 + 255) & ~255ull) +
+    const uint64_t head = ((plans_bytes + 255) & ~255ull) + 2 * (((uint64_t)na * 8 + 255) & ~255ull) +
                           ((((uint64_t)na + 1) * 8 + 255) & ~255ull) + (((uint64_t)na * 4 + 255) & ~255ull) +
                           ((rows_bytes + 255) & ~255ull);
     uint64_t budget = arena_cap;
@@ -1074,6 +1179,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     DQuery *d_plans = reinterpret_cast<DQuery *>(p);
     p += (plans_bytes + 255) & ~255ull;
     unsigned long long *d_counts = reinterpret_cast<unsigned long long *>(p);
+    p += ((uint64_t)na * 8 + 255) & ~255ull;
+    unsigned long long *d_step_counts = reinterpret_cast<unsigned long long *>(p);
     p += ((uint64_t)na * 8 + 255) & ~255ull;
     unsigned long long *d_rcoff = reinterpret_cast<unsigned long long *>(p);
     p += (((uint64_t)na + 1) * 8 + 255) & ~255ull;
@@ -1157,6 +1264,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
         c.root_coff = d_rcoff;
         c.root_cstart = d_rcstart;
+        c.counts = d_counts;
+        c.nq = na;
         c.max_scan = max_scan;
         c.max_candidates = lim.max_candidates;
         c.dmax = dmax;
@@ -1167,7 +1276,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.tile_parent = tile_parent;
         a.status = status;
         a.tile_ctr = tile_ctr;
-        a.counts = d_counts;
+        a.counts = d_step_counts;
         a.result = d_result;
         a.rows_out = d_rows;
         a.max_rows = max_rows;
@@ -1216,6 +1325,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0);
     std::vector<double> ratio(dmax + 1, 1.0);
+    std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
+    for (const DQuery &q : dq) has_final[q.k - 1] = 1;
     total[0] = rcoff[na];
     np[0] = na;
     uint32_t d = 0;
@@ -1232,7 +1343,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
             chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
         }
-        const uint32_t ntiles = (uint32_t)div_up(chunk, TILE);
+        const uint32_t vtile = variant_tile(variant);
+        const uint32_t ntiles = (uint32_t)div_up(chunk, vtile);
         if (++epoch >= (1u << 30)) {
             ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));
             epoch = 1;
@@ -1267,16 +1379,15 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.status = status;
         a.epoch = epoch;
         a.tile_ctr = tile_ctr;
-        a.counts = d_counts;
+        a.counts = d_step_counts;
         a.result = d_result;
         a.rows_out = d_rows;
         a.max_rows = max_rows;
         a.rows_ctr = rows_ctr;
-        k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, stream>>>(
-            a.pcoff, a.np, a.c0, chunk, ntiles, tile_parent, tile_ctr, d_result);
+        k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, na), 256), 256, 0, stream>>>(
+            a.pcoff, a.np, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts, na);
         ECHECK(cudaEventRecord(ev0, stream));
-        if (d == 0) k_step<true><<<ntiles, T, 0, stream>>>(a);
-        else k_step<false><<<ntiles, T, 0, stream>>>(a);
+        launch_step(variant, d == 0, a, ntiles, stream);
         ECHECK(cudaGetLastError());
         ECHECK(cudaEventRecord(ev1, stream));
         ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
@@ -1300,6 +1411,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (trace)
             fprintf(stderr, "gfsm-step depth=%u cand=%llu children=%llu next=%llu tiles=%u ms=%.4f\n", d, chunk,
                     emits ? r.n_children : 0ull, emits ? r.total_next : 0ull, ntiles, ms);
+        if (has_final[d])
+            k_commit<<<(unsigned)div_up(na, 256), 256, 0, stream>>>(d_counts, d_step_counts, na);
         st.candidates += chunk;
         st.expansions += r.n_children;
         if (lim.max_candidates && st.candidates > lim.max_candidates) {
@@ -1337,6 +1450,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     for (uint32_t i = 0; i < na; ++i) st.count += cnt[i];
     st.kernel_ms = kms;
+    st.tile_variant = variant;
     {
         float dms = 0.f;
         cudaEventElapsedTime(&dms, ev_begin, ev_end);
@@ -1527,10 +1641,11 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         a.counts = d_count;
         a.result = d_result;
         a.rows_ctr = rows_ctr;
-        k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(a.pcoff, a.np, a.c0, chunk, ntiles,
-                                                                                 tile_parent, tile_ctr, d_result);
-        if (d == 0) k_step<true><<<ntiles, T, 0, st>>>(a);
-        else k_step<false><<<ntiles, T, 0, st>>>(a);
+        // one query: a step either counts (last level) or emits, so a re-run
+        // step never counts twice and the count goes straight to the total
+        k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(
+            a.pcoff, a.np, a.c0, chunk, ntiles, TILE, tile_parent, tile_ctr, d_result, nullptr, 0);
+        launch_step(0, d == 0, a, ntiles, st);
         if (cudaGetLastError() != cudaSuccess) return GFSM_ERR_CUDA;
         StepResult r;
         if (cudaMemcpyAsync(&r, d_result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -45,9 +46,13 @@ struct Engine {
     gfsm_status build_graph(std::string &err);
     // Counts every plan against g; counts_out[i] for plans[i].  With rows_out
     // (single plan only) also writes up to max_rows full mappings.
+    // variant < 0: tile geometry chosen by the autotuner.
     gfsm_status run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                     uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
-                    uint64_t *n_rows, std::string &err);
+                    uint64_t *n_rows, std::string &err, int variant = -1);
+    int pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
+                     std::string &err);
+    std::map<uint64_t, int> tuned;  // autotuner: workload class -> tile geometry
 };
 
 }  // namespace gfsm

@@ -86,6 +86,7 @@ typedef struct {
     double   wall_ms;            /* host wall time of the call                     */
     uint64_t h2d_bytes;          /* host->device bytes copied by the call          */
     uint64_t d2h_bytes;          /* device->host bytes copied by the call          */
+    int32_t  tile_variant;       /* tile geometry the autotuner chose (0..3)        */
 } gfsm_stats;
 
 typedef struct {

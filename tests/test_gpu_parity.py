@@ -278,3 +278,80 @@ def test_device_and_host_drivers_agree(monkeypatch):
         assert c1 == c2 and s1["candidates"] == s2["candidates"]
     assert host_st["steps"] > 20
     ctx.close()
+
+
+@pytest.mark.parametrize("variant", ["0", "1", "2", "3"])
+def test_tile_geometries_agree(monkeypatch, variant):
+    """Every tile geometry the autotuner can pick gives the same counts,
+    candidates and expansions (hub rows, vertex labels and chunking)."""
+    monkeypatch.setenv("GFSM_TILE", variant)
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1, mem_limit=512 << 20)
+    g = synth.rmat(12, 25000, seed=6)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=7)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
+    dpath_plans = []
+    for i in range(24):
+        qg, _ = synth.rw_query(g, 3 + i % 4, tree=i % 2 == 0, seed=300 + i)
+        qs, qd = qg.directed()
+        dpath_plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    counts, st = ctx.batch_count(dpath_plans, data)
+    assert st["tile_variant"] == int(variant)
+    ref = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    monkeypatch.setenv("GFSM_TILE", "0")
+    rdata = ref.graph_from_edges(g.n, s, d, None, g.vlabel)
+    rplans = []
+    for i in range(24):
+        qg, _ = synth.rw_query(g, 3 + i % 4, tree=i % 2 == 0, seed=300 + i)
+        qs, qd = qg.directed()
+        rplans.append(ref.pre_process_query(ref.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    rcounts, rst = ref.batch_count(rplans, rdata)
+    assert counts.tolist() == rcounts.tolist() and counts.sum() > 0
+    tri = ctx.pre_process_query(ctx.file_parse(_g("queries/_3_triangle")))
+    udata = gfsm_b200.GFSM(device=0)
+    monkeypatch.setenv("GFSM_TILE", variant)
+    ud = udata.graph_from_edges(g.n, s, d)
+    assert udata.solve(udata.file_parse(_g("queries/_3_triangle")), ud) == 6 * O.triangles(g.n, g.src, g.dst)
+    ctx.close()
+    ref.close()
+    udata.close()
+
+
+def test_autotuner_choice_is_exact(monkeypatch):
+    monkeypatch.delenv("GFSM_TILE", raising=False)
+    ctx = gfsm_b200.GFSM(device=0)
+    g = synth.ba(5000, 4, seed=12)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d)
+    tri = ctx.pre_process_query(ctx.file_parse(_g("queries/_3_triangle")))
+    c, st = ctx.match_count(tri, data)
+    assert 0 <= st["tile_variant"] < 4
+    assert c == 6 * O.triangles(g.n, g.src, g.dst)
+    ctx.close()
+
+
+def test_mixed_batch_retries_count_once():
+    """A batch mixing query sizes under tight MEMLIMITs re-runs steps that
+    overflow their level buffer; queries that end at such a step must still be
+    counted once (per-step count scratch, committed on acceptance)."""
+    g = synth.grid(200, 0.05, 0.05, seed=21)
+    g.vlabel = synth.vlabels(g.n, 2, 0.0, seed=22)
+    s, d = g.directed()
+    results = []
+    for mem in (None, 24 << 20, 16 << 20, 12 << 20, 10 << 20):
+        kw = {} if mem is None else dict(mem_limit=mem, max_scan_size=1 << 16)
+        ctx = gfsm_b200.GFSM(device=0, vertex_labels=1, **kw)
+        data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
+        plans = []
+        for i in range(60):
+            qg, _ = synth.rw_query(g, 3 + i % 6, tree=i % 3 == 0, seed=700 + i)
+            qs, qd = qg.directed()
+            plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+        counts, st = ctx.batch_count(plans, data)
+        results.append((counts.tolist(), st["retries"], st["steps"]))
+        ctx.close()
+    ref = results[0][0]
+    assert sum(ref) > 0
+    for counts, retries, steps in results[1:]:
+        assert counts == ref
+    assert max(r for _, r, _ in results[1:]) > 0, [(r, st) for _, r, st in results]
