@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "engine.h"
@@ -146,6 +147,14 @@ struct StepArgs {
     uint32_t *rows_out;
     uint64_t max_rows;
     uint32_t *rows_ctr;
+    // shared query prefixes: root parents are entities root_base + i; a class
+    // entity stands for csize[e] member queries members[mstart[e] ..]; the
+    // fan-out step maps each candidate to (member, row offset)
+    uint32_t root_base;
+    uint32_t fanout;
+    const uint32_t *__restrict__ csize;
+    const uint32_t *__restrict__ mstart;
+    const uint32_t *__restrict__ members;
 };
 
 // Also zeroes the step's per-query count scratch: final-level counts of a
@@ -202,7 +211,7 @@ __device__ __forceinline__ V warp_sum(V x) {
 // coalesced write pass: parent index, candidate, and the child's own
 // next-level candidate slice (start, then its exclusive prefix in the tile).
 struct Stage {
-    uint32_t p, v, cs, cnt;
+    uint32_t p, v, cs, cnt, q;
 };
 
 // First index in a[0, n) with a[i] >= key, searched by a whole warp: 32
@@ -238,7 +247,7 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
 }
 
 constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
-constexpr int REQ_SMEM = 1024;      // entries staged per requirement row
+constexpr int REQ_SMEM = 768;       // entries staged per requirement row
 
 // Tile geometry of a level-step instantiation: threads per CTA, candidates
 // per thread, and the CTAs per SM its register budget is fitted to.
@@ -312,7 +321,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
 
     // ---- a tile inside one parent's slice (hub rows): stage the part of each
     // requirement row that can hold this tile's candidates
-    const bool single = !ROOT && plo == phi && a.g.elab == nullptr;
+    const bool single = !ROOT && plo == phi && a.g.elab == nullptr && !a.fanout;
     if (single) {
         const uint32_t q0 = ldf<P>(a.ptup + plo);
         const DLevel *L0 = &a.plans[q0].lv[d];
@@ -344,7 +353,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
         }
     }
-    if (tid == 0) sm.q0 = ROOT ? plo : ldf<P>(a.ptup + plo);
+    if (tid == 0) sm.q0 = ROOT ? a.root_base + plo : ldf<P>(a.ptup + plo);
     __syncthreads();
 
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
@@ -355,7 +364,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     for (int j = 0; j < CPT; ++j) {
         const unsigned long long c = base + (unsigned long long)(warp * WC + j * 32) + lane;
         bool emit = false;
-        Stage rec{0, 0, 0, 0};
+        Stage rec{0, 0, 0, 0, 0};
         if (c < tend) {
             // parent = largest p in [plo, phi] with coff[p] <= c
             uint32_t lo = 0, hi = nwin - 1;
@@ -372,8 +381,17 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             }
             const uint32_t p = plo + lo;
             const unsigned long long pc = win_smem ? sm.coff[lo] : ldf<P>(a.pcoff + p);
-            const uint32_t local = (uint32_t)(c - pc);
-            const uint32_t q = ROOT ? p : ldf<P>(a.ptup + p);
+            uint32_t local = (uint32_t)(c - pc);
+            uint32_t q = ROOT ? a.root_base + p : ldf<P>(a.ptup + p);
+            if (!ROOT && a.fanout) {
+                // a shared class tuple: candidates run over (member, row offset)
+                const uint32_t size = __ldg(a.csize + q);
+                const unsigned long long pn = win_smem ? sm.coff[lo + 1] : ldf<P>(a.pcoff + p + 1);
+                const uint32_t slen = (uint32_t)((pn - pc) / size);
+                const uint32_t j = local / slen;
+                local -= j * slen;
+                q = __ldg(a.members + __ldg(a.mstart + q) + j);
+            }
             const DLevel *L = &a.plans[q].lv[d];
             uint32_t v;
             bool pass = true;
@@ -452,7 +470,9 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
                         L->next_hi < a.g.n ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_hi) : re;
                     if (e > s) {  // a child with no candidates cannot be extended: not written
                         emit = true;
-                        rec = Stage{p, v, s, e - s};
+                        // a shared class's child offers its slice to every member
+                        const uint32_t cnt = L->fanout_next ? (e - s) * __ldg(a.csize + q) : e - s;
+                        rec = Stage{p, v, s, cnt, q};
                     }
                 }
             }
@@ -601,8 +621,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         const Stage r = sm.stage[w * WC + (i - sm.wofs[w])];
         const uint64_t slot = ex_cnt + i;
         if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
-        const uint32_t q = ROOT ? r.p : ldf<P>(a.ptup + r.p);
-        a.ctup[slot] = q;
+        a.ctup[slot] = r.q;
         for (uint32_t k = 0; k < d; ++k)
             a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = ldf<P>(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
         a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = r.v;
@@ -661,8 +680,8 @@ struct Ctl {
     StepArgs args;               // the step in flight (static fields preset by the host)
     const unsigned long long *root_coff;
     const uint32_t *root_cstart;
-    unsigned long long *counts;        // per-query totals (args.counts is the step scratch)
-    uint32_t nq, accepted;
+    unsigned long long *counts;        // per-entity totals (args.counts is the step scratch)
+    uint32_t nq, accepted, share_depth;
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
     uint32_t d, dmax, emits, done, epoch, err;
@@ -720,6 +739,7 @@ __device__ void ctl_plan(Ctl &c) {
         a.ccoff = nullptr;
     }
     a.epoch = ++c.epoch;
+    a.fanout = c.share_depth && d == c.share_depth;
     c.chunk = chunk;
     c.emits = emits;
     *a.tile_ctr = 0;
@@ -1166,37 +1186,99 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     const uint64_t rows_bytes = rows_out ? max_rows * (uint64_t)dq[0].k * 4 : 0;
 
-    // arena layout: plans | counts | root coff | root cstart | mapping rows | depth buffers
-    const uint64_t plans_bytes = (uint64_t)na * sizeof(DQuery);
-    const uint64_t head = ((plans_bytes + 255) & ~255ull) + 2 * (((uint64_t)na * 8 + 255) & ~255ull) +
-                          ((((uint64_t)na + 1) * 8 + 255) & ~255ull) + (((uint64_t)na * 4 + 255) & ~255ull) +
-                          ((rows_bytes + 255) & ~255ull);
+    // Shared prefixes: queries whose device plans for depths 0 and 1 are
+    // byte-identical (windows, requirements, final flags and the depth-2
+    // slice) form a class; depths 0 and 1 run once per class and the depth-2
+    // step fans each class tuple out to its members.  Entities are the
+    // queries [0, na) followed by the classes [na, na + ncls).
+    const char *shr = getenv("GFSM_SHARE");
+    const bool share = !rows_out && na >= 2 && dmax >= 2 && !(shr && *shr == '0');
+    std::vector<DQuery> ent(dq);
+    std::vector<uint32_t> csize(na, 1), mstart(na, 0), members, root_lo, root_hi;
+    std::vector<std::vector<uint32_t>> cls_members;
+    uint32_t root_base = 0;
+    if (share) {
+        std::map<std::string, uint32_t> cls;
+        for (uint32_t i = 0; i < na; ++i) {
+            const std::string key(reinterpret_cast<const char *>(&dq[i].lv[0]), 2 * sizeof(DLevel));
+            auto it = cls.find(key);
+            if (it == cls.end()) {
+                it = cls.emplace(key, (uint32_t)cls_members.size()).first;
+                cls_members.emplace_back();
+            }
+            cls_members[it->second].push_back(i);
+        }
+        root_base = na;
+        for (const auto &mem : cls_members) {
+            DQuery cq = dq[mem[0]];
+            if (cq.k > 2) cq.lv[1].fanout_next = 1;
+            ent.push_back(cq);
+            csize.push_back((uint32_t)mem.size());
+            mstart.push_back((uint32_t)members.size());
+            members.insert(members.end(), mem.begin(), mem.end());
+            root_lo.push_back(rlo[mem[0]]);
+            root_hi.push_back(rhi[mem[0]]);
+        }
+    } else {
+        root_lo = rlo;
+        root_hi = rhi;
+    }
+    const uint32_t ne = (uint32_t)ent.size();       // entities
+    const uint32_t nr = (uint32_t)root_lo.size();   // root-level parents
+    if (members.empty()) members.push_back(0);
+
+    // arena layout: plans | counts | step counts | root coff | root cstart |
+    //               class sizes | member starts | members | mapping rows | depth buffers
+    auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
+    const uint64_t plans_bytes = (uint64_t)ne * sizeof(DQuery);
+    const uint64_t head = al(plans_bytes) + 2 * al((uint64_t)ne * 8) + al(((uint64_t)nr + 1) * 8) +
+                          al((uint64_t)nr * 4) + 2 * al((uint64_t)ne * 4) + al((uint64_t)members.size() * 4) +
+                          al(rows_bytes);
     uint64_t budget = arena_cap;
     if (budget <= head + (1ull << 20) * dmax) return GFSM_ERR_NOMEM;
     gfsm_status rc = ensure_arena(budget, err);
     if (rc != GFSM_OK) return rc;
     char *p = static_cast<char *>(arena);
     DQuery *d_plans = reinterpret_cast<DQuery *>(p);
-    p += (plans_bytes + 255) & ~255ull;
+    p += al(plans_bytes);
     unsigned long long *d_counts = reinterpret_cast<unsigned long long *>(p);
-    p += ((uint64_t)na * 8 + 255) & ~255ull;
+    p += al((uint64_t)ne * 8);
     unsigned long long *d_step_counts = reinterpret_cast<unsigned long long *>(p);
-    p += ((uint64_t)na * 8 + 255) & ~255ull;
+    p += al((uint64_t)ne * 8);
     unsigned long long *d_rcoff = reinterpret_cast<unsigned long long *>(p);
-    p += (((uint64_t)na + 1) * 8 + 255) & ~255ull;
+    p += al(((uint64_t)nr + 1) * 8);
     uint32_t *d_rcstart = reinterpret_cast<uint32_t *>(p);
-    p += ((uint64_t)na * 4 + 255) & ~255ull;
+    p += al((uint64_t)nr * 4);
+    uint32_t *d_csize = reinterpret_cast<uint32_t *>(p);
+    p += al((uint64_t)ne * 4);
+    uint32_t *d_mstart = reinterpret_cast<uint32_t *>(p);
+    p += al((uint64_t)ne * 4);
+    uint32_t *d_members = reinterpret_cast<uint32_t *>(p);
+    p += al((uint64_t)members.size() * 4);
     uint32_t *d_rows = rows_out ? reinterpret_cast<uint32_t *>(p) : nullptr;
-    p += (rows_bytes + 255) & ~255ull;
+    p += al(rows_bytes);
 
-    std::vector<unsigned long long> rcoff(na + 1, 0);
-    for (uint32_t i = 0; i < na; ++i) rcoff[i + 1] = rcoff[i] + (rhi[i] - rlo[i]);
-    ECHECK(cudaMemcpyAsync(d_plans, dq.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemsetAsync(d_counts, 0, (uint64_t)na * 8, stream));
-    ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)na + 1) * 8, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_rcstart, rlo.data(), (uint64_t)na * 4, cudaMemcpyHostToDevice, stream));
+    std::vector<unsigned long long> rcoff(nr + 1, 0);
+    for (uint32_t i = 0; i < nr; ++i) rcoff[i + 1] = rcoff[i] + (root_hi[i] - root_lo[i]);
+    ECHECK(cudaMemcpyAsync(d_plans, ent.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemsetAsync(d_counts, 0, (uint64_t)ne * 8, stream));
+    ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)nr + 1) * 8, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_rcstart, root_lo.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_csize, csize.data(), (uint64_t)ne * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_mstart, mstart.data(), (uint64_t)ne * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_members, members.data(), (uint64_t)members.size() * 4, cudaMemcpyHostToDevice,
+                           stream));
     ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
-    st.h2d_bytes += plans_bytes + ((uint64_t)na + 1) * 8 + (uint64_t)na * 4;
+    st.h2d_bytes += plans_bytes + ((uint64_t)nr + 1) * 8 + (uint64_t)nr * 4 + (uint64_t)ne * 8 +
+                    (uint64_t)members.size() * 4;
+    // per-query totals from the per-entity counts: a class that ends at a
+    // shared depth counted once for all of its members
+    auto gather_counts = [&](const std::vector<unsigned long long> &cnt) {
+        std::vector<unsigned long long> out(cnt.begin(), cnt.begin() + na);
+        for (size_t c = 0; c < cls_members.size(); ++c)
+            for (uint32_t m : cls_members[c]) out[m] += cnt[na + c];
+        return out;
+    };
     ECHECK(cudaEventRecord(ev_begin, stream));
 
     // depth buffers 0 .. dmax-1 (depth dmax is count-only)
@@ -1253,8 +1335,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
         Ctl c;
         std::memset(&c, 0, sizeof(c));
-        c.total[0] = rcoff[na];
-        c.np[0] = na;
+        c.total[0] = rcoff[nr];
+        c.np[0] = nr;
         for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = 1.0f;
         for (uint32_t i = 0; i < dmax; ++i) {
             c.tup[i] = buf[i].tup;
@@ -1265,7 +1347,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         c.root_coff = d_rcoff;
         c.root_cstart = d_rcstart;
         c.counts = d_counts;
-        c.nq = na;
+        c.nq = ne;
+        c.share_depth = share ? 2 : 0;
         c.max_scan = max_scan;
         c.max_candidates = lim.max_candidates;
         c.dmax = dmax;
@@ -1281,6 +1364,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_out = d_rows;
         a.max_rows = max_rows;
         a.rows_ctr = rows_ctr;
+        a.root_base = root_base;
+        a.csize = d_csize;
+        a.mstart = d_mstart;
+        a.members = d_members;
         Ctl *d_ctl = static_cast<Ctl *>(ctl);
         ECHECK(cudaMemcpyAsync(d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         st.h2d_bytes += sizeof(Ctl);
@@ -1288,10 +1375,11 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         ECHECK(cudaGraphLaunch(graph_exec, stream));
         ECHECK(cudaEventRecord(ev1, stream));
         ECHECK(cudaMemcpyAsync(&c, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
-        std::vector<unsigned long long> cnt(na);
-        ECHECK(cudaMemcpyAsync(cnt.data(), d_counts, (uint64_t)na * 8, cudaMemcpyDeviceToHost, stream));
+        std::vector<unsigned long long> ecnt(ne);
+        ECHECK(cudaMemcpyAsync(ecnt.data(), d_counts, (uint64_t)ne * 8, cudaMemcpyDeviceToHost, stream));
         ECHECK(cudaStreamSynchronize(stream));
-        st.d2h_bytes += sizeof(Ctl) + (uint64_t)na * 8;
+        st.d2h_bytes += sizeof(Ctl) + (uint64_t)ne * 8;
+        const std::vector<unsigned long long> cnt = gather_counts(ecnt);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         epoch = c.epoch;
@@ -1327,8 +1415,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<double> ratio(dmax + 1, 1.0);
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) has_final[q.k - 1] = 1;
-    total[0] = rcoff[na];
-    np[0] = na;
+    total[0] = rcoff[nr];
+    np[0] = nr;
     uint32_t d = 0;
     float kms = 0.f;
     for (;;) {
@@ -1384,8 +1472,13 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_out = d_rows;
         a.max_rows = max_rows;
         a.rows_ctr = rows_ctr;
-        k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, na), 256), 256, 0, stream>>>(
-            a.pcoff, a.np, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts, na);
+        a.root_base = root_base;
+        a.fanout = share && d == 2;
+        a.csize = d_csize;
+        a.mstart = d_mstart;
+        a.members = d_members;
+        k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, ne), 256), 256, 0, stream>>>(
+            a.pcoff, a.np, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts, ne);
         ECHECK(cudaEventRecord(ev0, stream));
         launch_step(variant, d == 0, a, ntiles, stream);
         ECHECK(cudaGetLastError());
@@ -1412,7 +1505,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             fprintf(stderr, "gfsm-step depth=%u cand=%llu children=%llu next=%llu tiles=%u ms=%.4f\n", d, chunk,
                     emits ? r.n_children : 0ull, emits ? r.total_next : 0ull, ntiles, ms);
         if (has_final[d])
-            k_commit<<<(unsigned)div_up(na, 256), 256, 0, stream>>>(d_counts, d_step_counts, na);
+            k_commit<<<(unsigned)div_up(ne, 256), 256, 0, stream>>>(d_counts, d_step_counts, ne);
         st.candidates += chunk;
         st.expansions += r.n_children;
         if (lim.max_candidates && st.candidates > lim.max_candidates) {
@@ -1434,11 +1527,12 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
     }
     ECHECK(cudaEventRecord(ev_end, stream));
-    std::vector<unsigned long long> cnt(na);
-    ECHECK(cudaMemcpyAsync(cnt.data(), d_counts, (uint64_t)na * 8, cudaMemcpyDeviceToHost, stream));
-    st.d2h_bytes += (uint64_t)na * 8;
+    std::vector<unsigned long long> ecnt(ne);
+    ECHECK(cudaMemcpyAsync(ecnt.data(), d_counts, (uint64_t)ne * 8, cudaMemcpyDeviceToHost, stream));
+    st.d2h_bytes += (uint64_t)ne * 8;
     if (rows_out) ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
     ECHECK(cudaStreamSynchronize(stream));
+    const std::vector<unsigned long long> cnt = gather_counts(ecnt);
     for (uint32_t i = 0; i < na; ++i) counts_out[active[i]] = cnt[i];
     if (rows_out) {
         uint64_t total_rows = 0;

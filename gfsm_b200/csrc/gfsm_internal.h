@@ -79,7 +79,8 @@ struct alignas(16) DLevel {
     uint8_t anchor_lab;        // label of the anchor requirement
     uint8_t final_;            // depth == k-1
     uint8_t anchor_check;      // anchor requirement needs a row search (multi-edge data)
-    uint8_t pad0, pad1;
+    uint8_t fanout_next;       // depth+1 fans a shared class out to its member queries
+    uint8_t pad1;
     uint8_t req_pos[MAXQ];     // tuple position, or REQ_SELF
     uint8_t req_lab[MAXQ];
 };

@@ -355,3 +355,31 @@ def test_mixed_batch_retries_count_once():
     for counts, retries, steps in results[1:]:
         assert counts == ref
     assert max(r for _, r, _ in results[1:]) > 0, [(r, st) for _, r, st in results]
+
+
+def test_shared_prefix_batches(monkeypatch):
+    """Queries whose first two levels coincide share them (one class tuple
+    per shared partial mapping, fanned out to every member at depth 2); the
+    counts must equal unshared batching and one-at-a-time matching, on both
+    drivers, including members that end at a shared depth."""
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    g = synth.grid(150, 0.05, 0.03, seed=31)
+    g.vlabel = synth.vlabels(g.n, 2, 0.0, seed=32)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
+    plans = []
+    for i in range(200):
+        qg, _ = synth.rw_query(g, 2 + i % 7, tree=i % 4 == 0, seed=900 + i)
+        qs, qd = qg.directed()
+        plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    single = [ctx.match_count(p, data)[0] for p in plans]
+    monkeypatch.setenv("GFSM_SHARE", "0")
+    unshared, st0 = ctx.batch_count(plans, data)
+    monkeypatch.setenv("GFSM_SHARE", "1")
+    shared, st1 = ctx.batch_count(plans, data)
+    monkeypatch.setenv("GFSM_DRIVER", "graph")
+    shared_g, st2 = ctx.batch_count(plans, data)
+    assert unshared.tolist() == single == shared.tolist() == shared_g.tolist()
+    assert st1["candidates"] < st0["candidates"]  # levels 0 and 1 ran once per class
+    assert sum(single) > 0
+    ctx.close()
