@@ -1121,7 +1121,7 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
         return v >= 0 && v < kVariants ? v : 0;
     }
     const char *at = getenv("GFSM_AUTOTUNE");
-    if (at && *at == '0') return 0;
+    if (!autotune || (at && *at == '0')) return 0;
     uint32_t kmax = 0;
     for (const Plan *p : plans) kmax = std::max(kmax, p->k);
     const double avg = g.n ? (double)g.m / (double)g.n : 0.0;
@@ -1132,12 +1132,19 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
     const size_t ns = std::min<size_t>(plans.size(), 32);
     std::vector<const Plan *> sample(plans.begin(), plans.begin() + ns);
     std::vector<uint64_t> cnt(ns);
+    // Samples under 2 ms of device time are launch-bound and their timings
+    // mostly noise: keep the default there.  Elsewhere another geometry must
+    // beat the default by 3% to be chosen.
     int best = 0;
-    double best_ms = 1e300;
+    double base_ms = 0.0, best_ms = 1e300;
     for (int v = 0; v < kVariants; ++v) {
         gfsm_stats s{};
         if (run(sample, g, lim, cnt.data(), &s, nullptr, 0, nullptr, err, v) != GFSM_OK) return 0;
-        if (s.device_ms < best_ms) {
+        if (v == 0) {
+            base_ms = s.device_ms;
+            if (base_ms < 2.0) break;
+        }
+        if (s.device_ms < best_ms && (v == 0 || s.device_ms < 0.97 * base_ms)) {
             best_ms = s.device_ms;
             best = v;
         }

@@ -53,6 +53,7 @@ struct Engine {
     int pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                      std::string &err);
     std::map<uint64_t, int> tuned;  // autotuner: workload class -> tile geometry
+    bool autotune = true;           // off for served slots: tuning runs would sit on the request path
 };
 
 }  // namespace gfsm

@@ -149,6 +149,7 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         rc = e->init(ctx->device, 0, scan, err);
         if (rc != GFSM_OK) return rc;
         e->arena_cap = per_slot > e->small_bytes ? per_slot - e->small_bytes : 0;
+        e->autotune = false;  // a request never waits for tuning runs
         s->engines.push_back(std::move(e));
     }
     s->slot_budget = c.frontier_bytes ? c.frontier_bytes : per_slot;
