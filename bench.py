@@ -254,6 +254,24 @@ def run_ours(args, rank, world, local, pg):
         return out
 
     plans = plans_from_host()
+
+    # -- text ingest: the drop-in path parses `t # / v / e` text and builds the
+    # device CCSR (the reference parses serially on the host)
+    ingest = None
+    if rank == 0:
+        import tempfile
+        tpath = os.path.join(tempfile.mkdtemp(), "grid.g")
+        g.write_text(tpath)
+        size = os.path.getsize(tpath)
+        t0 = time.perf_counter()
+        tg = ctx.file_parse(tpath)
+        t1 = time.perf_counter()
+        tg.to_device()
+        t2 = time.perf_counter()
+        ingest = {"bytes": size, "parse_s": t1 - t0, "device_build_s": t2 - t1,
+                  "parse_mb_per_s": size / (t1 - t0) / 1e6, "threads": os.cpu_count()}
+        tg.close()
+        os.unlink(tpath)
     import torch
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -385,7 +403,7 @@ def run_ours(args, rank, world, local, pg):
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
-            "clocks": clk, "gpu_launches": launches,
+            "clocks": clk, "gpu_launches": launches, "ingest": ingest,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -261,7 +261,7 @@ using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
 using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
 using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
 constexpr int kVariants = 4;
-constexpr uint32_t kMinTile = 512;
+constexpr uint32_t kMinTile = 512;   // tile-status capacity is sized for this tile
 __host__ __device__ constexpr uint32_t variant_tile(int v) {
     return v == 0 ? Geo0::TILE : v == 1 ? Geo1::TILE : v == 2 ? Geo2::TILE : Geo3::TILE;
 }
@@ -299,6 +299,202 @@ __device__ __forceinline__ unsigned long long ldf(const unsigned long long *p) {
     unsigned long long v;
     asm volatile("ld.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
     return v;
+}
+
+// Decoupled look-back of one tile (called by one full warp): publishes the
+// tile's aggregate (child count, next-level candidate count), sums the
+// predecessors' values until an inclusive prefix is found, publishes its own
+// inclusive prefix, and returns the exclusive prefix.  Tiles are taken in
+// launch order, so every predecessor is running or done; each wait is
+// bounded by SPIN_LIMIT and reports KERR_LOOKBACK.  The last tile of the step
+// records the step's totals.
+__device__ __forceinline__ void tile_lookback(const StepArgs &a, const uint32_t tile, const uint32_t agg_cnt,
+                                              const unsigned long long agg_deg, const uint32_t lane,
+                                              unsigned long long &ex_cnt, unsigned long long &ex_deg) {
+    ex_cnt = 0;
+    ex_deg = 0;
+    TileStatus *st = a.status;
+    if (tile == 0) {
+        if (lane == 0) {
+            st[0].inc_deg = agg_deg;
+            st_release(&st[0].word, status_word(a.epoch, FLAG_INC, agg_cnt));
+        }
+    } else {
+        if (lane == 0) {
+            st[tile].agg_deg = agg_deg;
+            st_release(&st[tile].word, status_word(a.epoch, FLAG_AGG, agg_cnt));
+        }
+        long long pred = (long long)tile - 1;
+        uint32_t spins = 0;
+        bool failed = false;
+        for (;;) {
+            const long long idx = pred - (long long)lane;
+            unsigned long long w = 0;
+            uint32_t flag = FLAG_INC;
+            for (;;) {
+                if (idx >= 0) {
+                    w = ld_acquire(&st[idx].word);
+                    flag = (uint32_t)(w >> 34) == a.epoch ? (uint32_t)(w >> 32) & 3u : 0u;
+                }
+                if (__all_sync(0xffffffffu, flag != 0)) break;
+                if (++spins > SPIN_LIMIT) { failed = true; break; }
+                __nanosleep(64);
+            }
+            if (failed) break;
+            const uint32_t incm = __ballot_sync(0xffffffffu, flag == FLAG_INC);
+            const int first = incm ? __ffs(incm) - 1 : 32;
+            unsigned long long vc = 0, vd = 0;
+            if ((int)lane <= first && idx >= 0) {
+                vc = (uint32_t)w;
+                vd = flag == FLAG_INC ? __ldcg(&st[idx].inc_deg) : __ldcg(&st[idx].agg_deg);
+            }
+            ex_cnt += warp_sum(vc);
+            ex_deg += warp_sum(vd);
+            if (incm) break;
+            pred -= 32;
+        }
+        if (lane == 0) {
+            if (failed) atomicOr(&a.result->err, KERR_LOOKBACK);
+            st[tile].inc_deg = ex_deg + agg_deg;
+            st_release(&st[tile].word, status_word(a.epoch, FLAG_INC, (uint32_t)(ex_cnt + agg_cnt)));
+        }
+    }
+    if (lane == 0 && tile == a.ntiles - 1) {
+        a.result->n_children = ex_cnt + agg_cnt;
+        a.result->total_next = ex_deg + agg_deg;
+        if (ex_cnt + agg_cnt <= a.ccap) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
+    }
+}
+
+// Per-tile context of the candidate check: the parents' candidate prefix
+// window (shared memory, or null to search global memory), and for a tile
+// inside one parent's slice the staged requirement-row slices.
+struct CandCtx {
+    const unsigned long long *win;
+    uint32_t nwin, plo;
+    bool single;
+    const uint32_t *req;
+    uint32_t req_stride;
+    const uint32_t *rlo, *rhi, *rmode;
+};
+
+// One candidate c of a level step: find its parent, check it (injectivity,
+// anchor label, remaining requirements), and either count it (last query
+// vertex) or describe the child it becomes (emit, rec).
+template <bool ROOT, bool P>
+__device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_t d, const unsigned long long c,
+                                                const CandCtx &t, bool &emit, Stage &rec,
+                                                unsigned long long &my_bytes, uint32_t &fq, unsigned long long &fc) {
+    // parent = largest p in [plo, phi] with coff[p] <= c
+    uint32_t lo = 0, hi = t.nwin - 1;
+    if (t.win) {
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (t.win[mid] <= c) lo = mid; else hi = mid;
+        }
+    } else {
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            if (ldf<P>(a.pcoff + t.plo + mid) <= c) lo = mid; else hi = mid;
+        }
+    }
+    const uint32_t p = t.plo + lo;
+    const unsigned long long pc = t.win ? t.win[lo] : ldf<P>(a.pcoff + p);
+    uint32_t local = (uint32_t)(c - pc);
+    uint32_t q = ROOT ? a.root_base + p : ldf<P>(a.ptup + p);
+    if (!ROOT && a.fanout) {
+        // a shared class tuple: candidates run over (member, row offset)
+        const uint32_t size = __ldg(a.csize + q);
+        const unsigned long long pn = t.win ? t.win[lo + 1] : ldf<P>(a.pcoff + p + 1);
+        const uint32_t slen = (uint32_t)((pn - pc) / size);
+        const uint32_t j = local / slen;
+        local -= j * slen;
+        q = __ldg(a.members + __ldg(a.mstart + q) + j);
+    }
+    const DLevel *L = &a.plans[q].lv[d];
+    uint32_t v;
+    bool pass = true;
+    if (ROOT) {
+        v = ldf<P>(a.pcstart + p) + local;
+        my_bytes += 4;  // degree/label read of a data vertex
+    } else {
+        const uint32_t idx = ldf<P>(a.pcstart + p) + local;
+        v = __ldg(a.g.adj + idx);
+        if (L->anchor_check)
+            pass = has_edge(a.g, ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
+        else if (a.g.elab)
+            pass = __ldg(a.g.elab + idx) == L->anchor_lab;
+        // injectivity (HnGPU.cu:223-236)
+        for (uint32_t i = 0; i < d; ++i)
+            if (ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+        if (local == 0) {
+            // algorithmic bytes of this parent: its tuple and every backward
+            // neighbour's row (anchor + requirement rows), read once
+            const uint32_t anchor = ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
+            unsigned long long b = 4ull * d;
+            b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
+            for (uint32_t r = 0; r < L->nreq; ++r) {
+                const uint32_t pos = L->req_pos[r];
+                if (pos == REQ_SELF) continue;
+                const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
+            }
+            my_bytes += b;
+        }
+    }
+    // remaining requirements (HnGPU.cu:243-252)
+    for (uint32_t r = 0; r < L->nreq && pass; ++r) {
+        const uint32_t mode = (t.single && r < (uint32_t)NSTAGE) ? t.rmode[r] : 0u;
+        if (mode == 1u) {
+            const uint32_t n = t.rhi[r] - t.rlo[r];
+            const uint32_t k = smem_lower_bound(t.req + r * t.req_stride, n, v);
+            pass = k < n && t.req[r * t.req_stride + k] == v && L->req_lab[r] == a.g.single_label;
+        } else if (mode == 2u) {
+            const uint32_t n = t.rhi[r] - t.rlo[r];
+            const uint32_t k = lower_bound_u32(a.g.adj + t.rlo[r], n, v);
+            pass = k < n && __ldg(a.g.adj + t.rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
+        } else {
+            const uint32_t pos = L->req_pos[r];
+            const uint32_t u =
+                pos == REQ_SELF ? v : ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+            pass = has_edge(a.g, u, v, L->req_lab[r]);
+        }
+    }
+    if (pass) {
+        if (L->final_) {
+            if (a.rows_out) {
+                const uint32_t slot = atomicAdd(a.rows_ctr, 1u);
+                if (slot < a.max_rows) {
+                    const DQuery *Q = &a.plans[q];
+                    uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
+                    for (uint32_t i = 0; i < d; ++i)
+                        row[Q->col[i]] =
+                            __ldg(a.g.order + ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
+                    row[Q->col[d]] = __ldg(a.g.order + v);
+                }
+            }
+            if (fc && q != fq) {
+                atomicAdd(&a.counts[fq], fc);
+                fc = 0;
+            }
+            fq = q;
+            ++fc;
+        } else {
+            // the child's own candidate slice for depth+1
+            const uint32_t na = L->next_anchor;
+            const uint32_t w = na == d ? v : ldf<P>(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+            const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
+            const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
+            const uint32_t e =
+                L->next_hi < a.g.n ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_hi) : re;
+            if (e > s) {  // a child with no candidates cannot be extended: not written
+                emit = true;
+                // a shared class's child offers its slice to every member
+                const uint32_t cnt = L->fanout_next ? (e - s) * __ldg(a.csize + q) : e - s;
+                rec = Stage{p, v, s, cnt, q};
+            }
+        }
+    }
 }
 
 // One tile of a level step: candidates [c0 + tile*TILE, ...) of the step.
@@ -359,124 +555,15 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
     uint32_t fq = 0xffffffffu, wcnt = 0;
     Stage *wstage = sm.stage + warp * WC;
+    const CandCtx tctx{win_smem ? sm.coff : nullptr, nwin, plo, single, &sm.req[0][0], (uint32_t)REQ_SMEM,
+                       sm.rlo, sm.rhi, sm.rmode};
 
 #pragma unroll 1
     for (int j = 0; j < CPT; ++j) {
         const unsigned long long c = base + (unsigned long long)(warp * WC + j * 32) + lane;
         bool emit = false;
         Stage rec{0, 0, 0, 0, 0};
-        if (c < tend) {
-            // parent = largest p in [plo, phi] with coff[p] <= c
-            uint32_t lo = 0, hi = nwin - 1;
-            if (win_smem) {
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (sm.coff[mid] <= c) lo = mid; else hi = mid;
-                }
-            } else {
-                while (hi - lo > 1) {
-                    const uint32_t mid = lo + ((hi - lo) >> 1);
-                    if (ldf<P>(a.pcoff + plo + mid) <= c) lo = mid; else hi = mid;
-                }
-            }
-            const uint32_t p = plo + lo;
-            const unsigned long long pc = win_smem ? sm.coff[lo] : ldf<P>(a.pcoff + p);
-            uint32_t local = (uint32_t)(c - pc);
-            uint32_t q = ROOT ? a.root_base + p : ldf<P>(a.ptup + p);
-            if (!ROOT && a.fanout) {
-                // a shared class tuple: candidates run over (member, row offset)
-                const uint32_t size = __ldg(a.csize + q);
-                const unsigned long long pn = win_smem ? sm.coff[lo + 1] : ldf<P>(a.pcoff + p + 1);
-                const uint32_t slen = (uint32_t)((pn - pc) / size);
-                const uint32_t j = local / slen;
-                local -= j * slen;
-                q = __ldg(a.members + __ldg(a.mstart + q) + j);
-            }
-            const DLevel *L = &a.plans[q].lv[d];
-            uint32_t v;
-            bool pass = true;
-            if (ROOT) {
-                v = ldf<P>(a.pcstart + p) + local;
-                my_bytes += 4;  // degree/label read of a data vertex
-            } else {
-                const uint32_t idx = ldf<P>(a.pcstart + p) + local;
-                v = __ldg(a.g.adj + idx);
-                if (L->anchor_check)
-                    pass = has_edge(a.g, ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
-                else if (a.g.elab)
-                    pass = __ldg(a.g.elab + idx) == L->anchor_lab;
-                // injectivity (HnGPU.cu:223-236)
-                for (uint32_t i = 0; i < d; ++i)
-                    if (ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
-                if (local == 0) {
-                    // algorithmic bytes of this parent: its tuple and every backward
-                    // neighbour's row (anchor + requirement rows), read once
-                    const uint32_t anchor = ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
-                    unsigned long long b = 4ull * d;
-                    b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
-                    for (uint32_t r = 0; r < L->nreq; ++r) {
-                        const uint32_t pos = L->req_pos[r];
-                        if (pos == REQ_SELF) continue;
-                        const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                        b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
-                    }
-                    my_bytes += b;
-                }
-            }
-            // remaining requirements (HnGPU.cu:243-252)
-            for (uint32_t r = 0; r < L->nreq && pass; ++r) {
-                const uint32_t mode = (single && r < (uint32_t)NSTAGE) ? sm.rmode[r] : 0u;
-                if (mode == 1u) {
-                    const uint32_t n = sm.rhi[r] - sm.rlo[r];
-                    const uint32_t k = smem_lower_bound(sm.req[r], n, v);
-                    pass = k < n && sm.req[r][k] == v && L->req_lab[r] == a.g.single_label;
-                } else if (mode == 2u) {
-                    const uint32_t n = sm.rhi[r] - sm.rlo[r];
-                    const uint32_t k = lower_bound_u32(a.g.adj + sm.rlo[r], n, v);
-                    pass = k < n && __ldg(a.g.adj + sm.rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
-                } else {
-                    const uint32_t pos = L->req_pos[r];
-                    const uint32_t u =
-                        pos == REQ_SELF ? v : ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                    pass = has_edge(a.g, u, v, L->req_lab[r]);
-                }
-            }
-            if (pass) {
-                if (L->final_) {
-                    if (a.rows_out) {
-                        const uint32_t slot = atomicAdd(a.rows_ctr, 1u);
-                        if (slot < a.max_rows) {
-                            const DQuery *Q = &a.plans[q];
-                            uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
-                            for (uint32_t i = 0; i < d; ++i)
-                                row[Q->col[i]] =
-                                    __ldg(a.g.order + ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
-                            row[Q->col[d]] = __ldg(a.g.order + v);
-                        }
-                    }
-                    if (fc && q != fq) {
-                        atomicAdd(&a.counts[fq], fc);
-                        fc = 0;
-                    }
-                    fq = q;
-                    ++fc;
-                } else {
-                    // the child's own candidate slice for depth+1
-                    const uint32_t na = L->next_anchor;
-                    const uint32_t w = na == d ? v : ldf<P>(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
-                    const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-                    const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
-                    const uint32_t e =
-                        L->next_hi < a.g.n ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_hi) : re;
-                    if (e > s) {  // a child with no candidates cannot be extended: not written
-                        emit = true;
-                        // a shared class's child offers its slice to every member
-                        const uint32_t cnt = L->fanout_next ? (e - s) * __ldg(a.csize + q) : e - s;
-                        rec = Stage{p, v, s, cnt, q};
-                    }
-                }
-            }
-        }
+        if (c < tend) check_candidate<ROOT, P>(a, d, c, tctx, emit, rec, my_bytes, fq, fc);
         if (emits) {
             const uint32_t bal = __ballot_sync(0xffffffffu, emit);
             if (emit) wstage[wcnt + __popc(bal & ((1u << lane) - 1u))] = rec;
@@ -552,63 +639,11 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     __syncthreads();
     // ---- decoupled look-back (warp 0)
     if (warp == 0) {
-        const uint32_t agg_cnt = (uint32_t)sm.agg_cnt;
-        const unsigned long long agg_deg = sm.agg_deg;
         unsigned long long ex_cnt = 0, ex_deg = 0;
-        TileStatus *st = a.status;
-        if (tile == 0) {
-            if (lane == 0) {
-                st[0].inc_deg = agg_deg;
-                st_release(&st[0].word, status_word(a.epoch, FLAG_INC, agg_cnt));
-            }
-        } else {
-            if (lane == 0) {
-                st[tile].agg_deg = agg_deg;
-                st_release(&st[tile].word, status_word(a.epoch, FLAG_AGG, agg_cnt));
-            }
-            long long pred = (long long)tile - 1;
-            uint32_t spins = 0;
-            bool failed = false;
-            for (;;) {
-                const long long idx = pred - (long long)lane;
-                unsigned long long w = 0;
-                uint32_t flag = FLAG_INC;
-                for (;;) {
-                    if (idx >= 0) {
-                        w = ld_acquire(&st[idx].word);
-                        flag = (uint32_t)(w >> 34) == a.epoch ? (uint32_t)(w >> 32) & 3u : 0u;
-                    }
-                    if (__all_sync(0xffffffffu, flag != 0)) break;
-                    if (++spins > SPIN_LIMIT) { failed = true; break; }
-                    __nanosleep(64);
-                }
-                if (failed) break;
-                const uint32_t incm = __ballot_sync(0xffffffffu, flag == FLAG_INC);
-                const int first = incm ? __ffs(incm) - 1 : 32;
-                unsigned long long vc = 0, vd = 0;
-                if ((int)lane <= first && idx >= 0) {
-                    vc = (uint32_t)w;
-                    vd = flag == FLAG_INC ? __ldcg(&st[idx].inc_deg) : __ldcg(&st[idx].agg_deg);
-                }
-                ex_cnt += warp_sum(vc);
-                ex_deg += warp_sum(vd);
-                if (incm) break;
-                pred -= 32;
-            }
-            if (lane == 0) {
-                if (failed) atomicOr(&a.result->err, KERR_LOOKBACK);
-                st[tile].inc_deg = ex_deg + agg_deg;
-                st_release(&st[tile].word, status_word(a.epoch, FLAG_INC, (uint32_t)(ex_cnt + agg_cnt)));
-            }
-        }
+        tile_lookback(a, tile, (uint32_t)sm.agg_cnt, sm.agg_deg, lane, ex_cnt, ex_deg);
         if (lane == 0) {
             sm.excl_cnt = ex_cnt;
             sm.excl_deg = ex_deg;
-            if (tile == a.ntiles - 1) {
-                a.result->n_children = ex_cnt + agg_cnt;
-                a.result->total_next = ex_deg + agg_deg;
-                if (ex_cnt + agg_cnt <= a.ccap) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
-            }
         }
     }
     __syncthreads();
@@ -638,6 +673,8 @@ __global__ void __launch_bounds__(G::T, G::MINB) k_step(const StepArgs a) {
     __syncthreads();
     step_tile<ROOT, false, G>(a, s_tile, sm);
 }
+
+
 
 // Launches one level step with the given tile geometry.
 void launch_step(int variant, bool root, const StepArgs &a, uint32_t ntiles, cudaStream_t st) {
@@ -1439,6 +1476,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
         }
         const uint32_t vtile = variant_tile(variant);
+        chunk = std::min<unsigned long long>(chunk, (unsigned long long)status_tiles * vtile);
         const uint32_t ntiles = (uint32_t)div_up(chunk, vtile);
         if (++epoch >= (1u << 30)) {
             ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));

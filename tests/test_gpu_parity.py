@@ -330,10 +330,12 @@ def test_autotuner_choice_is_exact(monkeypatch):
     ctx.close()
 
 
-def test_mixed_batch_retries_count_once():
+def test_mixed_batch_retries_count_once(monkeypatch):
     """A batch mixing query sizes under tight MEMLIMITs re-runs steps that
     overflow their level buffer; queries that end at such a step must still be
-    counted once (per-step count scratch, committed on acceptance)."""
+    counted once (per-step count scratch, committed on acceptance).  A CTA-tile
+    geometry is pinned: its steps are large enough to overflow."""
+    monkeypatch.setenv("GFSM_TILE", "0")
     g = synth.grid(200, 0.05, 0.05, seed=21)
     g.vlabel = synth.vlabels(g.n, 2, 0.0, seed=22)
     s, d = g.directed()
