@@ -45,20 +45,6 @@ namespace {
 constexpr int T = 256;
 constexpr int CPT = 4;
 constexpr int TILE = T * CPT;
-constexpr uint32_t FLAG_AGG = 1, FLAG_INC = 2;
-constexpr uint32_t SPIN_LIMIT = 1u << 22;
-
-__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ unsigned long long status_word(uint32_t epoch, uint32_t flag, uint32_t cnt) {
-    return ((unsigned long long)epoch << 34) | ((unsigned long long)flag << 32) | cnt;
-}
 
 // First index in a[0, n) whose value is >= key (branch-free halving).
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
@@ -136,10 +122,7 @@ struct StepArgs {
     uint64_t cstride, ccap;
     uint32_t *ccstart;
     unsigned long long *ccoff;                      // [ccap+1]
-    // look-back
-    TileStatus *status;
-    uint32_t epoch;
-    uint32_t *tile_ctr;
+    uint32_t *tile_ctr;                             // tile queue of the fixed-grid step kernel
     // results
     unsigned long long *counts;                     // per query
     StepResult *result;
@@ -168,11 +151,7 @@ __global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_
     for (uint32_t i = t; i < nq; i += gridDim.x * blockDim.x) step_counts[i] = 0;
     if (t == 0) {
         *tile_ctr = 0;
-        result->n_children = 0;
-        result->total_next = 0;
-        result->alg_bytes = 0;
-        result->err = 0;
-        result->rows = 0;
+        *result = StepResult{};
     }
     if (t > ntiles) return;
     const unsigned long long c = c0 + (t < ntiles ? (unsigned long long)t * tile_size : ncand - 1);
@@ -261,7 +240,7 @@ using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
 using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
 using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
 constexpr int kVariants = 4;
-constexpr uint32_t kMinTile = 512;   // tile-status capacity is sized for this tile
+constexpr uint32_t kMinTile = 512;   // the tile directory is sized for this tile
 __host__ __device__ constexpr uint32_t variant_tile(int v) {
     return v == 0 ? Geo0::TILE : v == 1 ? Geo1::TILE : v == 2 ? Geo2::TILE : Geo3::TILE;
 }
@@ -276,93 +255,32 @@ struct StepSmem {
     uint32_t wcnt[G::NWARP], wofs[G::NWARP + 1];
     unsigned long long wdeg[G::NWARP], wdofs[G::NWARP], wbytes[G::NWARP];
     uint32_t q0, vfirst, vlast;
-    unsigned long long excl_cnt, excl_deg, agg_cnt, agg_deg, fcount;
+    unsigned long long excl_cnt, excl_deg, fcount;
 };
 
-// Loads of frontier data (parent tuples, slice starts, candidate prefixes,
-// the tile directory).  A kernel launch per step may read them through the
-// read-only (non-coherent) path.  The persistent kernel rewrites these
-// buffers within one launch, so it must not: it uses ordinary weak loads,
-// which its grid barrier (release by every writer, acquire by every reader)
-// makes observe the previous step's writes.  The asm keeps the compiler from
-// turning them into read-only-path loads.
-template <bool P>
-__device__ __forceinline__ uint32_t ldf(const uint32_t *p) {
-    if (!P) return __ldg(p);
-    uint32_t v;
-    asm volatile("ld.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
-    return v;
-}
-template <bool P>
-__device__ __forceinline__ unsigned long long ldf(const unsigned long long *p) {
-    if (!P) return *p;
-    unsigned long long v;
-    asm volatile("ld.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
-    return v;
-}
-
-// Decoupled look-back of one tile (called by one full warp): publishes the
-// tile's aggregate (child count, next-level candidate count), sums the
-// predecessors' values until an inclusive prefix is found, publishes its own
-// inclusive prefix, and returns the exclusive prefix.  Tiles are taken in
-// launch order, so every predecessor is running or done; each wait is
-// bounded by SPIN_LIMIT and reports KERR_LOOKBACK.  The last tile of the step
-// records the step's totals.
-__device__ __forceinline__ void tile_lookback(const StepArgs &a, const uint32_t tile, const uint32_t agg_cnt,
-                                              const unsigned long long agg_deg, const uint32_t lane,
-                                              unsigned long long &ex_cnt, unsigned long long &ex_deg) {
-    ex_cnt = 0;
-    ex_deg = 0;
-    TileStatus *st = a.status;
-    if (tile == 0) {
-        if (lane == 0) {
-            st[0].inc_deg = agg_deg;
-            st_release(&st[0].word, status_word(a.epoch, FLAG_INC, agg_cnt));
-        }
-    } else {
-        if (lane == 0) {
-            st[tile].agg_deg = agg_deg;
-            st_release(&st[tile].word, status_word(a.epoch, FLAG_AGG, agg_cnt));
-        }
-        long long pred = (long long)tile - 1;
-        uint32_t spins = 0;
-        bool failed = false;
-        for (;;) {
-            const long long idx = pred - (long long)lane;
-            unsigned long long w = 0;
-            uint32_t flag = FLAG_INC;
-            for (;;) {
-                if (idx >= 0) {
-                    w = ld_acquire(&st[idx].word);
-                    flag = (uint32_t)(w >> 34) == a.epoch ? (uint32_t)(w >> 32) & 3u : 0u;
-                }
-                if (__all_sync(0xffffffffu, flag != 0)) break;
-                if (++spins > SPIN_LIMIT) { failed = true; break; }
-                __nanosleep(64);
-            }
-            if (failed) break;
-            const uint32_t incm = __ballot_sync(0xffffffffu, flag == FLAG_INC);
-            const int first = incm ? __ffs(incm) - 1 : 32;
-            unsigned long long vc = 0, vd = 0;
-            if ((int)lane <= first && idx >= 0) {
-                vc = (uint32_t)w;
-                vd = flag == FLAG_INC ? __ldcg(&st[idx].inc_deg) : __ldcg(&st[idx].agg_deg);
-            }
-            ex_cnt += warp_sum(vc);
-            ex_deg += warp_sum(vd);
-            if (incm) break;
-            pred -= 32;
-        }
-        if (lane == 0) {
-            if (failed) atomicOr(&a.result->err, KERR_LOOKBACK);
-            st[tile].inc_deg = ex_deg + agg_deg;
-            st_release(&st[tile].word, status_word(a.epoch, FLAG_INC, (uint32_t)(ex_cnt + agg_cnt)));
-        }
-    }
-    if (lane == 0 && tile == a.ntiles - 1) {
-        a.result->n_children = ex_cnt + agg_cnt;
-        a.result->total_next = ex_deg + agg_deg;
-        if (ex_cnt + agg_cnt <= a.ccap) a.ccoff[ex_cnt + agg_cnt] = ex_deg + agg_deg;
+// Child slots of one tile (called by one thread): a single atomic on the
+// step's allocator takes agg_cnt consecutive slots and the matching range of
+// the next level's candidate prefix, so no tile waits for another.  Slot
+// order across tiles is the order of their atomics.  The tile that allocates
+// last publishes the step's totals and the prefix's closing entry.
+__device__ __forceinline__ void tile_alloc(const StepArgs &a, const unsigned long long agg_cnt,
+                                           const unsigned long long agg_deg, unsigned long long &ex_cnt,
+                                           unsigned long long &ex_deg) {
+    StepResult *r = a.result;
+    const bool big = agg_deg > kAllocMask;
+    const unsigned long long old =
+        agg_cnt ? atomicAdd(&r->alloc, (agg_cnt << kAllocShift) + (big ? 0ull : agg_deg)) : 0ull;
+    ex_cnt = old >> kAllocShift;
+    ex_deg = old & kAllocMask;
+    if (big || ex_deg + agg_deg > kAllocMask) atomicOr(&r->next_ovf, 1u);  // the host redoes a smaller chunk
+    __threadfence();  // this tile's allocation is visible before it counts as done
+    if (atomicAdd(&r->tiles_done, 1u) == a.ntiles - 1) {
+        __threadfence();
+        const unsigned long long tot = atomicAdd(&r->alloc, 0ull);
+        const unsigned long long n = tot >> kAllocShift, next = tot & kAllocMask;
+        r->n_children = n;
+        r->total_next = next;
+        if (n <= a.ccap) a.ccoff[n] = next;
     }
 }
 
@@ -381,7 +299,7 @@ struct CandCtx {
 // One candidate c of a level step: find its parent, check it (injectivity,
 // anchor label, remaining requirements), and either count it (last query
 // vertex) or describe the child it becomes (emit, rec).
-template <bool ROOT, bool P>
+template <bool ROOT>
 __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_t d, const unsigned long long c,
                                                 const CandCtx &t, bool &emit, Stage &rec,
                                                 unsigned long long &my_bytes, uint32_t &fq, unsigned long long &fc) {
@@ -395,17 +313,17 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
     } else {
         while (hi - lo > 1) {
             const uint32_t mid = lo + ((hi - lo) >> 1);
-            if (ldf<P>(a.pcoff + t.plo + mid) <= c) lo = mid; else hi = mid;
+            if (__ldg(a.pcoff + t.plo + mid) <= c) lo = mid; else hi = mid;
         }
     }
     const uint32_t p = t.plo + lo;
-    const unsigned long long pc = t.win ? t.win[lo] : ldf<P>(a.pcoff + p);
+    const unsigned long long pc = t.win ? t.win[lo] : __ldg(a.pcoff + p);
     uint32_t local = (uint32_t)(c - pc);
-    uint32_t q = ROOT ? a.root_base + p : ldf<P>(a.ptup + p);
+    uint32_t q = ROOT ? a.root_base + p : __ldg(a.ptup + p);
     if (!ROOT && a.fanout) {
         // a shared class tuple: candidates run over (member, row offset)
         const uint32_t size = __ldg(a.csize + q);
-        const unsigned long long pn = t.win ? t.win[lo + 1] : ldf<P>(a.pcoff + p + 1);
+        const unsigned long long pn = t.win ? t.win[lo + 1] : __ldg(a.pcoff + p + 1);
         const uint32_t slen = (uint32_t)((pn - pc) / size);
         const uint32_t j = local / slen;
         local -= j * slen;
@@ -415,28 +333,28 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
     uint32_t v;
     bool pass = true;
     if (ROOT) {
-        v = ldf<P>(a.pcstart + p) + local;
+        v = __ldg(a.pcstart + p) + local;
         my_bytes += 4;  // degree/label read of a data vertex
     } else {
-        const uint32_t idx = ldf<P>(a.pcstart + p) + local;
+        const uint32_t idx = __ldg(a.pcstart + p) + local;
         v = __ldg(a.g.adj + idx);
         if (L->anchor_check)
-            pass = has_edge(a.g, ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
+            pass = has_edge(a.g, __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
         else if (a.g.elab)
             pass = __ldg(a.g.elab + idx) == L->anchor_lab;
         // injectivity (HnGPU.cu:223-236)
         for (uint32_t i = 0; i < d; ++i)
-            if (ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+            if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
         if (local == 0) {
             // algorithmic bytes of this parent: its tuple and every backward
             // neighbour's row (anchor + requirement rows), read once
-            const uint32_t anchor = ldf<P>(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
+            const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
             unsigned long long b = 4ull * d;
             b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
             for (uint32_t r = 0; r < L->nreq; ++r) {
                 const uint32_t pos = L->req_pos[r];
                 if (pos == REQ_SELF) continue;
-                const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
                 b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
             }
             my_bytes += b;
@@ -456,7 +374,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
         } else {
             const uint32_t pos = L->req_pos[r];
             const uint32_t u =
-                pos == REQ_SELF ? v : ldf<P>(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
             pass = has_edge(a.g, u, v, L->req_lab[r]);
         }
     }
@@ -469,7 +387,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
                     uint32_t *row = a.rows_out + (uint64_t)slot * Q->k;
                     for (uint32_t i = 0; i < d; ++i)
                         row[Q->col[i]] =
-                            __ldg(a.g.order + ldf<P>(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
+                            __ldg(a.g.order + __ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p));
                     row[Q->col[d]] = __ldg(a.g.order + v);
                 }
             }
@@ -482,7 +400,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
         } else {
             // the child's own candidate slice for depth+1
             const uint32_t na = L->next_anchor;
-            const uint32_t w = na == d ? v : ldf<P>(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+            const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
             const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
             const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
             const uint32_t e =
@@ -498,7 +416,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
 }
 
 // One tile of a level step: candidates [c0 + tile*TILE, ...) of the step.
-template <bool ROOT, bool P, class G>
+template <bool ROOT, class G>
 __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile, StepSmem<G> &sm) {
     constexpr int T = G::T, CPT = G::CPT, TILE = G::TILE, WIN = G::WIN, NWARP = G::NWARP, WC = G::WC;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -507,11 +425,11 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     __syncthreads();
     const unsigned long long base = a.c0 + (unsigned long long)tile * TILE;
     const unsigned long long tend = min(base + (unsigned long long)TILE, a.cend);
-    const uint32_t plo = ldf<P>(a.tile_parent + tile), phi = ldf<P>(a.tile_parent + tile + 1);
+    const uint32_t plo = __ldg(a.tile_parent + tile), phi = __ldg(a.tile_parent + tile + 1);
     const uint32_t nwin = phi - plo + 2;  // coff[plo .. phi+1]
     const bool win_smem = nwin <= (uint32_t)WIN;
     if (win_smem)
-        for (uint32_t i = tid; i < nwin; i += T) sm.coff[i] = ldf<P>(a.pcoff + plo + i);
+        for (uint32_t i = tid; i < nwin; i += T) sm.coff[i] = __ldg(a.pcoff + plo + i);
     const uint32_t d = a.depth;
     const bool emits = a.ctup != nullptr;
 
@@ -519,11 +437,11 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     // requirement row that can hold this tile's candidates
     const bool single = !ROOT && plo == phi && a.g.elab == nullptr && !a.fanout;
     if (single) {
-        const uint32_t q0 = ldf<P>(a.ptup + plo);
+        const uint32_t q0 = __ldg(a.ptup + plo);
         const DLevel *L0 = &a.plans[q0].lv[d];
         if (tid == 0) {
-            const uint32_t cs0 = ldf<P>(a.pcstart + plo);
-            const unsigned long long c00 = ldf<P>(a.pcoff + plo);
+            const uint32_t cs0 = __ldg(a.pcstart + plo);
+            const unsigned long long c00 = __ldg(a.pcoff + plo);
             sm.vfirst = __ldg(a.g.adj + cs0 + (uint32_t)(base - c00));
             sm.vlast = __ldg(a.g.adj + cs0 + (uint32_t)(tend - 1 - c00));
         }
@@ -531,7 +449,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         if (warp < 2 * NSTAGE) {
             const uint32_t r = warp >> 1;
             if (r < L0->nreq && L0->req_pos[r] != REQ_SELF) {
-                const uint32_t u = ldf<P>(a.ptup + (uint64_t)(1 + L0->req_pos[r]) * a.pstride + plo);
+                const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + L0->req_pos[r]) * a.pstride + plo);
                 const uint32_t rs = __ldg(a.g.rowptr + u), re = __ldg(a.g.rowptr + u + 1);
                 const uint32_t key = (warp & 1) ? sm.vlast + 1 : sm.vfirst;
                 const uint32_t b = rs + warp_lower_bound(a.g.adj + rs, re - rs, key, lane);
@@ -549,7 +467,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
         }
     }
-    if (tid == 0) sm.q0 = ROOT ? a.root_base + plo : ldf<P>(a.ptup + plo);
+    if (tid == 0) sm.q0 = ROOT ? a.root_base + plo : __ldg(a.ptup + plo);
     __syncthreads();
 
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
@@ -563,7 +481,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         const unsigned long long c = base + (unsigned long long)(warp * WC + j * 32) + lane;
         bool emit = false;
         Stage rec{0, 0, 0, 0, 0};
-        if (c < tend) check_candidate<ROOT, P>(a, d, c, tctx, emit, rec, my_bytes, fq, fc);
+        if (c < tend) check_candidate<ROOT>(a, d, c, tctx, emit, rec, my_bytes, fq, fc);
         if (emits) {
             const uint32_t bal = __ballot_sync(0xffffffffu, emit);
             if (emit) wstage[wcnt + __popc(bal & ((1u << lane) - 1u))] = rec;
@@ -631,20 +549,12 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             bb += sm.wbytes[w];
         }
         sm.wofs[NWARP] = (uint32_t)cc;
-        sm.agg_cnt = cc;
-        sm.agg_deg = dd;
+        unsigned long long ex_cnt = 0, ex_deg = 0;
+        tile_alloc(a, cc, dd, ex_cnt, ex_deg);
+        sm.excl_cnt = ex_cnt;
+        sm.excl_deg = ex_deg;
         if (bb) atomicAdd(&a.result->alg_bytes, bb);
         if (sm.fcount) atomicAdd(&a.counts[sm.q0], sm.fcount);
-    }
-    __syncthreads();
-    // ---- decoupled look-back (warp 0)
-    if (warp == 0) {
-        unsigned long long ex_cnt = 0, ex_deg = 0;
-        tile_lookback(a, tile, (uint32_t)sm.agg_cnt, sm.agg_deg, lane, ex_cnt, ex_deg);
-        if (lane == 0) {
-            sm.excl_cnt = ex_cnt;
-            sm.excl_deg = ex_deg;
-        }
     }
     __syncthreads();
     // ---- write the tile's children: consecutive threads -> consecutive slots
@@ -658,7 +568,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
         a.ctup[slot] = r.q;
         for (uint32_t k = 0; k < d; ++k)
-            a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = ldf<P>(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
+            a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
         a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = r.v;
         a.ccstart[slot] = r.cs;
         a.ccoff[slot] = ex_deg + sm.wdofs[w] + r.cnt;
@@ -668,10 +578,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
 template <bool ROOT, class G>
 __global__ void __launch_bounds__(G::T, G::MINB) k_step(const StepArgs a) {
     __shared__ StepSmem<G> sm;
-    __shared__ uint32_t s_tile;
-    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);  // launch order: predecessors are running or done
-    __syncthreads();
-    step_tile<ROOT, false, G>(a, s_tile, sm);
+    step_tile<ROOT, G>(a, blockIdx.x, sm);
 }
 
 
@@ -699,11 +606,10 @@ void launch_step(int variant, bool root, const StepArgs &a, uint32_t ntiles, cud
 }
 
 // ---------------------------------------------------------------------------
-// Device-driven batch: one persistent cooperative launch runs the whole
-// depth-first schedule.  A fixed grid (every CTA resident) takes tiles from
-// a device counter -- the work queue -- and a controller in CTA 0 makes the
-// host loop's decisions (chunk size, retry on overflow, descend / return)
-// between grid barriers, so no step returns to the host.
+// Device-driven schedule: a CUDA graph whose WHILE node repeats (controller ->
+// tile directory -> level step).  The controller kernel makes the host loop's
+// decisions (chunk size, retry on overflow, descend / return) on the device,
+// so no step returns to the host.
 // ---------------------------------------------------------------------------
 static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
 
@@ -721,8 +627,7 @@ struct Ctl {
     uint32_t nq, accepted, share_depth;
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
-    uint32_t d, dmax, emits, done, epoch, err;
-    unsigned int bar_count, bar_gen;
+    uint32_t d, dmax, emits, done, err;
 };
 
 constexpr uint32_t KERR_CAP = 16u;      // max_candidates reached
@@ -745,6 +650,7 @@ __device__ void ctl_plan(Ctl &c) {
         const double allowed = (double)c.cap[d] / fmax((double)c.ratio[d], 1.0 / 8192.0);
         const unsigned long long lim = (unsigned long long)fmax(allowed, (double)TILE);
         if (chunk > lim) chunk = lim;
+        if (chunk > kMaxEmitChunk) chunk = kMaxEmitChunk;
     }
     StepArgs &a = c.args;
     a.depth = d;
@@ -775,15 +681,11 @@ __device__ void ctl_plan(Ctl &c) {
         a.ccstart = nullptr;
         a.ccoff = nullptr;
     }
-    a.epoch = ++c.epoch;
     a.fanout = c.share_depth && d == c.share_depth;
     c.chunk = chunk;
     c.emits = emits;
     *a.tile_ctr = 0;
-    StepResult *r = a.result;
-    r->n_children = r->total_next = r->alg_bytes = 0;
-    r->err = 0;
-    r->rows = 0;
+    *a.result = StepResult{};
 }
 
 // Accounts the finished step (the host loop's logic).
@@ -791,16 +693,18 @@ __device__ void ctl_after(Ctl &c) {
     const StepResult *rp = c.args.result;
     const unsigned long long n = __ldcg(&rp->n_children), next = __ldcg(&rp->total_next);
     const unsigned long long ab = __ldcg(&rp->alg_bytes);
-    const uint32_t e = __ldcg(&rp->err);
+    uint32_t e = __ldcg(&rp->err);
+    const uint32_t ovf = __ldcg(&rp->next_ovf);
     const uint32_t d = c.d;
     c.steps++;
     c.accepted = 0;
+    if (c.emits && ovf && c.chunk <= TILE) e |= KERR_CAP;  // one tile's children alone overflow
     if (e) {
         c.err |= e;
         c.done = 1;
         return;
     }
-    if (c.emits && n > c.cap[d]) {
+    if (c.emits && (n > c.cap[d] || ovf)) {
         c.retries++;
         c.ratio[d] = (float)fmax((double)c.ratio[d] * 4.0, 2.0 * (double)n / (double)c.chunk);
         return;
@@ -871,7 +775,7 @@ __global__ void k_part_g(int slot, const Ctl *ctl) {
 }
 
 // Graph node: the level step on a fixed grid; every CTA takes tiles from the
-// step's counter (in order, so the look-back only waits on running tiles).
+// step's tile queue.
 __global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g(int slot) {
     __shared__ StepSmem<Geo0> sm;
     __shared__ uint32_t s_tile;
@@ -881,8 +785,8 @@ __global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g(int slot) {
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= a.ntiles) break;
-        if (a.depth == 0) step_tile<true, false, Geo0>(a, tile, sm);
-        else step_tile<false, false, Geo0>(a, tile, sm);
+        if (a.depth == 0) step_tile<true, Geo0>(a, tile, sm);
+        else step_tile<false, Geo0>(a, tile, sm);
     }
 }
 
@@ -1037,15 +941,13 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     ECHECK(cudaEventCreate(&ev_end));
     ECHECK(cudaMallocHost(&h_result, sizeof(StepResult)));
     max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
-    status_tiles = (uint32_t)div_up(max_scan, kMinTile);
-    // small region: tile status, tile directory, counters, result, plans
-    small_bytes = (uint64_t)status_tiles * sizeof(TileStatus) + ((((uint64_t)status_tiles + 2) * 4 + 255) & ~255ull) +
-                  512 + ((sizeof(Ctl) + 255) & ~255ull);
+    dir_tiles = (uint32_t)div_up(max_scan, kMinTile);
+    // small region: result, counters, tile directory, schedule control block
+    small_bytes = 512 + ((((uint64_t)dir_tiles + 2) * 4 + 255) & ~255ull) + ((sizeof(Ctl) + 255) & ~255ull);
     ECHECK(cudaMalloc(&small, small_bytes));
     ECHECK(cudaMemsetAsync(small, 0, small_bytes, stream));
     char *p = static_cast<char *>(small);
-    status = reinterpret_cast<TileStatus *>(p);
-    p += (uint64_t)status_tiles * sizeof(TileStatus);
+    static_assert(sizeof(StepResult) <= 64, "StepResult fits its slot");
     d_result = reinterpret_cast<StepResult *>(p);
     p += 64;
     tile_ctr = reinterpret_cast<uint32_t *>(p);
@@ -1053,10 +955,9 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     rows_ctr = reinterpret_cast<uint32_t *>(p);
     p += 64;
     tile_parent = reinterpret_cast<uint32_t *>(p);
-    p += (((uint64_t)status_tiles + 2) * 4 + 255) & ~255ull;
+    p += (((uint64_t)dir_tiles + 2) * 4 + 255) & ~255ull;
     ctl = p;
     arena_cap = arena_limit;
-    epoch = 0;
     {
         int sms = 0, per_sm = 0;
         ECHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1373,10 +1274,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     const char *drv = getenv("GFSM_DRIVER");
     const bool graph_driver = !trace && drv && !strcmp(drv, "graph") && build_graph(err) == GFSM_OK;
     if (graph_driver) {
-        if (epoch > (1u << 30) - (1u << 24)) {
-            ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));
-            epoch = 0;
-        }
         Ctl c;
         std::memset(&c, 0, sizeof(c));
         c.total[0] = rcoff[nr];
@@ -1396,12 +1293,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         c.max_scan = max_scan;
         c.max_candidates = lim.max_candidates;
         c.dmax = dmax;
-        c.epoch = epoch;
         StepArgs &a = c.args;
         a.g = gv;
         a.plans = d_plans;
         a.tile_parent = tile_parent;
-        a.status = status;
         a.tile_ctr = tile_ctr;
         a.counts = d_step_counts;
         a.result = d_result;
@@ -1426,7 +1321,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         const std::vector<unsigned long long> cnt = gather_counts(ecnt);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
-        epoch = c.epoch;
         st.steps = c.steps;
         st.retries = c.retries;
         st.candidates = c.candidates;
@@ -1437,8 +1331,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (c.err) {
             err = "device schedule error bits " + std::to_string(c.err);
             if (stats) *stats = st;
-            if (c.err & KERR_CAP) return GFSM_ERR_TOO_LARGE;
-            return (c.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
+            return (c.err & KERR_CAP) ? GFSM_ERR_TOO_LARGE : GFSM_ERR_CUDA;
         }
         for (uint32_t i = 0; i < na; ++i) counts_out[active[i]] = cnt[i];
         if (rows_out) {
@@ -1474,14 +1367,11 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (emits) {
             const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
             chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
+            chunk = std::min<unsigned long long>(chunk, kMaxEmitChunk);
         }
         const uint32_t vtile = variant_tile(variant);
-        chunk = std::min<unsigned long long>(chunk, (unsigned long long)status_tiles * vtile);
+        chunk = std::min<unsigned long long>(chunk, (unsigned long long)dir_tiles * vtile);
         const uint32_t ntiles = (uint32_t)div_up(chunk, vtile);
-        if (++epoch >= (1u << 30)) {
-            ECHECK(cudaMemsetAsync(status, 0, (uint64_t)status_tiles * sizeof(TileStatus), stream));
-            epoch = 1;
-        }
         StepArgs a{};
         a.g = gv;
         a.plans = d_plans;
@@ -1509,8 +1399,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             a.ccstart = buf[d].cstart;
             a.ccoff = buf[d].coff;
         }
-        a.status = status;
-        a.epoch = epoch;
         a.tile_ctr = tile_ctr;
         a.counts = d_step_counts;
         a.result = d_result;
@@ -1538,10 +1426,15 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         const StepResult r = *h_result;
         if (r.err) {
             err = "device step error bits " + std::to_string(r.err);
-            return (r.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
+            return GFSM_ERR_CUDA;
         }
-        if (emits && r.n_children > buf[d].cap) {
-            // more survivors than the level buffer holds: redo a smaller chunk
+        if (emits && r.next_ovf && chunk <= vtile) {
+            err = "one tile's children have more next-level candidates than a step can index";
+            return GFSM_ERR_TOO_LARGE;
+        }
+        if (emits && (r.n_children > buf[d].cap || r.next_ovf)) {
+            // more survivors than the level buffer holds (or more next-level
+            // candidates than the allocator indexes): redo a smaller chunk
             st.retries++;
             ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
             continue;
@@ -1616,9 +1509,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
 // match then allocates nothing: no cudaMalloc / cudaFree / cudaMallocHost /
 // cudaMallocAsync, no stream or event creation.
 //
-// Limit: the scratch is kNoAllocScratchBytes (64 MiB) per device -- tile
-// status for steps of up to kNoAllocTiles * 1024 candidates plus a frontier
-// arena shared by the query's levels.  Queries always fit because the
+// Limit: the scratch is kNoAllocScratchBytes (64 MiB) per device -- the
+// tile directory for steps of up to kNoAllocTiles * 1024 candidates plus a
+// frontier arena shared by the query's levels.  Queries always fit because the
 // depth-first chunking shrinks steps to the arena; a query whose plan cannot
 // get even one tile of frontier per level is rejected with
 // GFSM_ERR_TOO_LARGE.  Every process that loads libgfsm.so holds this array
@@ -1634,7 +1527,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[kMaxDevices] = {};  // device address of the scratch, per device
-uint32_t g_noalloc_epoch[kMaxDevices] = {};
 
 }  // namespace
 
@@ -1659,11 +1551,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         void *addr = nullptr;
         if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return GFSM_ERR_CUDA;
         scratch = static_cast<unsigned char *>(addr);
-        // tile status words must not carry an epoch a later step could reuse
-        if (cudaMemsetAsync(scratch, 0, (uint64_t)kNoAllocTiles * sizeof(TileStatus), st) != cudaSuccess)
-            return GFSM_ERR_CUDA;
         g_noalloc_ptr[g.device] = scratch;
-        g_noalloc_epoch[g.device] = 0;
     }
 
     DQuery dq;
@@ -1674,11 +1562,9 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     if (never) return GFSM_OK;
     const uint32_t dmax = dq.k - 1;
 
-    // scratch layout: tile status | result | counters | tile directory |
+    // scratch layout: result | counters | tile directory |
     //                 plan | count | root coff | root slice start | depth buffers
     unsigned char *p = scratch;
-    TileStatus *status = reinterpret_cast<TileStatus *>(p);
-    p += (uint64_t)kNoAllocTiles * sizeof(TileStatus);
     StepResult *d_result = reinterpret_cast<StepResult *>(p);
     p += 256;
     uint32_t *tile_ctr = reinterpret_cast<uint32_t *>(p);
@@ -1730,7 +1616,6 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     total[0] = rc2[1];
     np[0] = 1;
     uint32_t d = 0;
-    uint32_t &epoch = g_noalloc_epoch[g.device];
     for (;;) {
         if (pos[d] >= total[d]) {
             if (d == 0) break;
@@ -1742,13 +1627,9 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         if (emits) {
             const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
             chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
+            chunk = std::min<unsigned long long>(chunk, kMaxEmitChunk);
         }
         const uint32_t ntiles = (uint32_t)div_up(chunk, TILE);
-        if (++epoch >= (1u << 30)) {
-            if (cudaMemsetAsync(status, 0, (uint64_t)kNoAllocTiles * sizeof(TileStatus), st) != cudaSuccess)
-                return GFSM_ERR_CUDA;
-            epoch = 1;
-        }
         StepArgs a{};
         a.g = gv;
         a.plans = d_plan;
@@ -1774,8 +1655,6 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
             a.ccstart = buf[d].cstart;
             a.ccoff = buf[d].coff;
         }
-        a.status = status;
-        a.epoch = epoch;
         a.tile_ctr = tile_ctr;
         a.counts = d_count;
         a.result = d_result;
@@ -1790,8 +1669,9 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         if (cudaMemcpyAsync(&r, d_result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return GFSM_ERR_CUDA;
-        if (r.err) return (r.err & KERR_LOOKBACK) ? GFSM_ERR_DEVICE_WAIT : GFSM_ERR_CUDA;
-        if (emits && r.n_children > buf[d].cap) {
+        if (r.err) return GFSM_ERR_CUDA;
+        if (emits && r.next_ovf && chunk <= TILE) return GFSM_ERR_TOO_LARGE;
+        if (emits && (r.n_children > buf[d].cap || r.next_ovf)) {
             ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
             continue;
         }

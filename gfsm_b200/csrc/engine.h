@@ -17,17 +17,15 @@ struct Engine {
     void *arena = nullptr;         // frontier buffers + per-call plans/counts
     uint64_t arena_bytes = 0;
     uint64_t arena_cap = 0;        // bytes the arena may use (MEMLIMIT share)
-    void *small = nullptr;         // tile status, tile directory, counters
+    void *small = nullptr;         // step result, counters, tile directory, control block
     uint64_t small_bytes = 0;
-    TileStatus *status = nullptr;
-    uint32_t status_tiles = 0;
+    uint32_t dir_tiles = 0;        // tile directory capacity (tiles per step)
     StepResult *d_result = nullptr;
     StepResult *h_result = nullptr;  // pinned
     uint32_t *tile_ctr = nullptr;
     uint32_t *rows_ctr = nullptr;
     uint32_t *tile_parent = nullptr;
     uint64_t max_scan = 0;
-    uint32_t epoch = 0;
     // graph-driven schedule (one graph launch per call; built once per engine)
     int arg_slot = -1;             // constant-memory slot for this engine's step arguments
     void *ctl = nullptr;           // device control block (inside the small region)

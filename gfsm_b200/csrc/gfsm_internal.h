@@ -93,24 +93,28 @@ struct alignas(16) DQuery {
     uint32_t pad[3];
 };
 
+// Totals of one level step.  `alloc` hands out child slots: every tile adds
+// (its children << kAllocShift) + (their next-level candidates) with one
+// atomic, so slot order and the candidate prefix advance together.
 struct StepResult {
     unsigned long long n_children;
     unsigned long long total_next;
     unsigned long long alg_bytes;
+    unsigned long long alloc;
     unsigned int err;          // KERR_* bits
     unsigned int rows;         // mapping rows claimed (mapping mode)
+    unsigned int tiles_done;   // tiles that have allocated (the last one publishes the totals)
+    unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
 };
 
-struct TileStatus {
-    unsigned long long word;   // epoch:30 | flag:2 | count:32
-    unsigned long long agg_deg;
-    unsigned long long inc_deg;
-    unsigned long long pad;
-};
+constexpr int kAllocShift = 38;                                  // child count: bits 38..63
+constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candidates: bits 0..37
+// An emitting step takes fewer candidates than the child-count field holds,
+// so the count never wraps (every candidate yields at most one child).
+constexpr unsigned long long kMaxEmitChunk = (1ull << (64 - kAllocShift)) - 1024;
 
 // Error bits raised by kernels (read by the host after each step).
 enum : uint32_t {
-    KERR_LOOKBACK = 1u,        // bounded look-back wait ran out
     KERR_WINDOW = 2u,          // parent window larger than expected
     KERR_BOUNDS = 4u,          // a vertex id out of range
 };

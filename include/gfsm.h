@@ -35,7 +35,7 @@ typedef enum {
     GFSM_ERR_CUDA = 301,         /* a CUDA runtime call failed */
     GFSM_ERR_NOMEM = 302,        /* MEMLIMIT too small for the graph or one frontier step */
     GFSM_ERR_TOO_LARGE = 303,    /* graph or query beyond the supported sizes */
-    GFSM_ERR_DEVICE_WAIT = 304,  /* a bounded device-side wait ran out (kernel returned early) */
+    GFSM_ERR_DEVICE_WAIT = 304,  /* reserved: a bounded device-side wait ran out (no kernel waits today) */
     GFSM_ERR_NO_EXTENSION = 305, /* no CUDA device / kernels unavailable */
     GFSM_ERR_BUSY = 306,         /* server queue full */
     GFSM_ERR_STOPPED = 307       /* server stopped */
