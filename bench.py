@@ -247,11 +247,8 @@ def run_ours(args, rank, world, local, pg):
     qdir = [(q.n,) + tuple(q.directed()) + (q.vlabel,) for q in qs]
 
     def plans_from_host():
-        out = []
-        for n, a, b, vl in qdir:
-            qg = ctx.graph_from_edges(n, a, b, None, vl)
-            out.append(ctx.pre_process_query(qg))
-        return out
+        # every query's edge list -> plan, in one C call
+        return ctx.prepare_queries((n, a, b, None, vl) for n, a, b, vl in qdir)
 
     plans = plans_from_host()
 

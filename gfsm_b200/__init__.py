@@ -212,6 +212,33 @@ class GFSM:
         self._check(self._lib.gfsm_query_prepare(self._h, query.handle, C.byref(h)))
         return Plan(self, h.value)
 
+    def prepare_queries(self, queries):
+        """Plans for many queries in one call (gfsm_query_prepare_batch).
+
+        queries: iterable of (n, src, dst, elabel or None, vlabel or None),
+        directed edge lists with ids local to each query.  The labels must be
+        given for all queries or for none."""
+        queries = list(queries)
+        nq = len(queries)
+        if nq == 0:
+            return []
+        nv = np.fromiter((int(q[0]) for q in queries), np.uint32, nq)
+        ne = np.fromiter((len(q[1]) for q in queries), np.uint64, nq)
+        eoff = np.zeros(nq + 1, np.uint64)
+        np.cumsum(ne, out=eoff[1:])
+        cat = lambda i: np.ascontiguousarray(np.concatenate([np.asarray(q[i], np.uint32) for q in queries]),
+                                             np.uint32) if queries[0][i] is not None else None
+        src, dst, el, vl = cat(1), cat(2), cat(3), cat(4)
+        ptr = lambda a: a.ctypes.data_as(_lib.u32p) if a is not None and len(a) else None
+        if src is not None and len(src) == 0:
+            src = dst = None
+        out = (C.c_void_p * nq)()
+        failed = C.c_int(-1)
+        self._check(self._lib.gfsm_query_prepare_batch(
+            self._h, nq, nv.ctypes.data_as(_lib.u32p), eoff.ctypes.data_as(_lib.u64p), ptr(src), ptr(dst),
+            ptr(el), ptr(vl), out, C.byref(failed)))
+        return [Plan(self, out[i]) for i in range(nq)]
+
     # -- matching -------------------------------------------------------------
     def match_count(self, plan, data):
         cnt = C.c_uint64()

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <thread>
 
 #include "engine.h"
 #include "gfsm_internal.h"
@@ -173,6 +174,25 @@ gfsm_status gfsm_graph_load_text(gfsm_ctx *ctx, const char *path, gfsm_graph **o
     return gfsm_graph_load_buffer(ctx, text.data(), text.size(), out);
 }
 
+// An edge list as a host graph; edge labels keep the relation bits the
+// reference's packed CCSR keeps (CCSRRelSize).
+static gfsm_status edges_to_host(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                                 const uint32_t *elabel, const uint32_t *vlabel, uint32_t rel_bits, HostGraph &h) {
+    h.n = n;
+    h.src.assign(src, src + m);
+    h.dst.assign(dst, dst + m);
+    h.lab.resize(m);
+    const uint32_t vb = 32u - rel_bits;
+    for (uint64_t i = 0; i < m; ++i) {
+        if (src[i] >= n || dst[i] >= n) return GFSM_ERR_INVALID_DATA;
+        const uint32_t l = elabel ? elabel[i] : 1u;
+        h.lab[i] = (uint8_t)(((uint32_t)(l << vb)) >> vb);
+    }
+    h.vlabel.assign(n, 0);
+    if (vlabel) std::memcpy(h.vlabel.data(), vlabel, (uint64_t)n * 4);
+    return GFSM_OK;
+}
+
 gfsm_status gfsm_graph_from_edges(gfsm_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
                                   const uint32_t *elabel, const uint32_t *vlabel, gfsm_graph **out) {
     if (!ctx || !out || (m && (!src || !dst))) return GFSM_ERR_ARG;
@@ -182,19 +202,8 @@ gfsm_status gfsm_graph_from_edges(gfsm_ctx *ctx, uint32_t n, uint64_t m, const u
     g->ctx = ctx;
     g->rel_bits = ctx->lim.ccsr_rel_size;
     g->vl_mode = ctx->lim.vertex_labels != 0;
-    HostGraph &h = g->h;
-    h.n = n;
-    h.src.assign(src, src + m);
-    h.dst.assign(dst, dst + m);
-    h.lab.resize(m);
-    const uint32_t vb = 32u - g->rel_bits;
-    for (uint64_t i = 0; i < m; ++i) {
-        if (src[i] >= n || dst[i] >= n) return set_err(ctx, GFSM_ERR_INVALID_DATA, "edge endpoint out of range");
-        const uint32_t l = elabel ? elabel[i] : 1u;
-        h.lab[i] = (uint8_t)(((uint32_t)(l << vb)) >> vb);
-    }
-    h.vlabel.assign(n, 0);
-    if (vlabel) std::memcpy(h.vlabel.data(), vlabel, (uint64_t)n * 4);
+    if (edges_to_host(n, m, src, dst, elabel, vlabel, g->rel_bits, g->h) != GFSM_OK)
+        return set_err(ctx, GFSM_ERR_INVALID_DATA, "edge endpoint out of range");
     *out = g.release();
     return GFSM_OK;
 }
@@ -266,6 +275,53 @@ gfsm_status gfsm_query_prepare(gfsm_ctx *ctx, const gfsm_graph *q, gfsm_plan **o
     gfsm_status rc = plan_query(q->h, q->rel_bits, p->p);
     if (rc != GFSM_OK) return set_err(ctx, rc, "");
     *out = p.release();
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, const uint64_t *eoff,
+                                     const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                                     const uint32_t *vlabel, gfsm_plan **out, int *failed) {
+    if (failed) *failed = -1;
+    if (!ctx || nq < 0 || (nq && (!nv || !eoff || !out))) return GFSM_ERR_ARG;
+    if (nq == 0) return GFSM_OK;
+    if (eoff[nq] && (!src || !dst)) return GFSM_ERR_ARG;
+    for (int i = 0; i < nq; ++i) {
+        out[i] = nullptr;
+        if (eoff[i + 1] < eoff[i] || eoff[i + 1] - eoff[i] >= (1ull << 32)) return GFSM_ERR_ARG;
+    }
+    std::vector<uint64_t> voff(nq + 1, 0);
+    for (int i = 0; i < nq; ++i) voff[i + 1] = voff[i] + nv[i];
+    const uint32_t rel_bits = ctx->lim.ccsr_rel_size;
+    std::vector<gfsm_status> rc(nq, GFSM_OK);
+    // queries are tiny: one worker per ~64 of them, up to the host's threads
+    const int hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min(hw, (nq + 63) / 64));
+    auto work = [&](int t) {
+        for (int i = t; i < nq; i += nt) {
+            HostGraph h;
+            const uint64_t e0 = eoff[i], m = eoff[i + 1] - e0;
+            rc[i] = edges_to_host(nv[i], m, src + e0, dst + e0, elabel ? elabel + e0 : nullptr,
+                                  vlabel ? vlabel + voff[i] : nullptr, rel_bits, h);
+            if (rc[i] != GFSM_OK) continue;
+            auto p = std::unique_ptr<gfsm_plan>(new (std::nothrow) gfsm_plan());
+            if (!p) { rc[i] = GFSM_ERR_NOMEM; continue; }
+            rc[i] = plan_query(h, rel_bits, p->p);
+            if (rc[i] == GFSM_OK) out[i] = p.release();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (int i = 0; i < nq; ++i)
+        if (rc[i] != GFSM_OK) {
+            for (int j = 0; j < nq; ++j) {
+                delete out[j];
+                out[j] = nullptr;
+            }
+            if (failed) *failed = i;
+            return set_err(ctx, rc[i], "query " + std::to_string(i) + " of the batch");
+        }
     return GFSM_OK;
 }
 

@@ -120,3 +120,53 @@ def test_matching_needs_a_device(host_ctx):
     with pytest.raises(gfsm_b200.GFSMError) as ei:
         host_ctx.solve(q, d)
     assert ei.value.status == 305
+
+
+def test_batch_planning_matches_one_at_a_time(host_ctx):
+    """gfsm_query_prepare_batch gives every query the plan gfsm_query_prepare
+    gives it (random walks of 3-12 vertices, with and without labels)."""
+    from gfsm_b200 import synth
+    g = synth.ba(2000, 3, seed=7)
+    g.vlabel = synth.vlabels(g.n, 4, 0.0, seed=3)
+    qs = []
+    for i in range(300):
+        qg, _ = synth.rw_query(g, 3 + i % 10, tree=i % 3 == 0, seed=100 + i)
+        a, b = qg.directed()
+        qs.append((qg.n, a, b, None, qg.vlabel))
+    for use_labels in (True, False):
+        batch = host_ctx.prepare_queries(q if use_labels else q[:4] + (None,) for q in qs)
+        assert len(batch) == len(qs)
+        for q, p in zip(qs, batch):
+            one = host_ctx.pre_process_query(host_ctx.graph_from_edges(q[0], q[1], q[2], None,
+                                                                       q[4] if use_labels else None))
+            t, r = p.tables(), one.tables()
+            for key in ("order", "header", "reqs"):
+                assert t[key].tolist() == r[key].tolist()
+            assert p.columns().tolist() == one.columns().tolist()
+
+
+def test_batch_planning_reports_the_failing_query(host_ctx):
+    """A disconnected query fails the whole batch with its own status (1) and
+    index; an edge endpoint out of range is invalid data."""
+    import ctypes as C
+    tri = (3, [0, 1, 1, 2, 2, 0], [1, 0, 2, 1, 0, 2], None, None)
+    split = (4, [0, 1, 2, 3], [1, 0, 3, 2], None, None)
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.prepare_queries([tri, tri, split, tri])
+    assert ei.value.status == 1
+    lib = host_ctx._lib
+    nv = np.array([3, 4], np.uint32)
+    eoff = np.array([0, 6, 10], np.uint64)
+    src = np.array(tri[1] + split[1], np.uint32)
+    dst = np.array(tri[2] + split[2], np.uint32)
+    out = (C.c_void_p * 2)()
+    failed = C.c_int(7)
+    rc = lib.gfsm_query_prepare_batch(host_ctx._h, 2, nv.ctypes.data_as(_lib.u32p), eoff.ctypes.data_as(_lib.u64p),
+                                      src.ctypes.data_as(_lib.u32p), dst.ctypes.data_as(_lib.u32p), None, None,
+                                      out, C.byref(failed))
+    assert rc == 1 and failed.value == 1 and out[0] is None and out[1] is None
+    bad = (3, [0, 1, 5], [1, 0, 0], None, None)
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.prepare_queries([tri, bad])
+    assert ei.value.status == 233  # GFSM_ERR_INVALID_DATA
+    assert host_ctx.prepare_queries([]) == []
