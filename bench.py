@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-at-a-time measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-planner", action="store_true", help="skip the data-aware-order measurement")
     return ap.parse_args()
 
 
@@ -317,6 +318,25 @@ def run_ours(args, rank, world, local, pg):
     assert counts2.tolist() == ref_counts.tolist()
     e2e = total_queries / t_e2e
 
+    # -- data-aware matching order (gfsm_query_prepare_for): the same counts;
+    # the headline above keeps the reference's order
+    planner = None
+    if not args.no_planner:
+        p3 = ctx.prepare_queries(((n, a, b, None, vl) for n, a, b, vl in qdir), data)
+        ms3 = []
+        for i in range(args.warmup + args.steps):
+            flush_l2()
+            counts3, st3 = ctx.batch_count(p3, data)
+            assert counts3.tolist() == ref_counts.tolist()
+            if i >= args.warmup:
+                ms3.append(st3["device_ms"])
+        planner = {"reference_order_ms": float(np.median(dev_ms)), "data_aware_ms": float(np.median(ms3)),
+                   "reference_order_candidates": int(st["candidates"]),
+                   "data_aware_candidates": int(st3["candidates"]),
+                   "data_aware_plans": int(sum(p.info()["planner"] for p in p3)), "exact": True}
+        for p in p3:
+            p.close()
+
     # -- plain form: one query at a time
     exact = True
     plain = None
@@ -400,7 +420,7 @@ def run_ours(args, rank, world, local, pg):
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
-            "clocks": clk, "gpu_launches": launches, "ingest": ingest,
+            "clocks": clk, "gpu_launches": launches, "ingest": ingest, "planner": planner,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

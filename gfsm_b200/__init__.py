@@ -115,6 +115,12 @@ class Plan:
                                               header.ctypes.data_as(_lib.u32p), reqs.ctypes.data_as(_lib.u32p)))
         return {"k": k, "max_valency": mv, "order": order, "header": header, "reqs": reqs[: 2 * mv * k]}
 
+    def info(self):
+        """{"planner": 0 reference order / 1 data-aware, "order_invariant": bool}"""
+        pl, inv = C.c_uint32(), C.c_uint32()
+        self._ctx._check(self._ctx._lib.gfsm_plan_info(self._h, C.byref(pl), C.byref(inv)))
+        return {"planner": pl.value, "order_invariant": bool(inv.value)}
+
     def columns(self):
         k = self.tables()["k"]
         cols = np.zeros(k, np.uint32)
@@ -212,12 +218,20 @@ class GFSM:
         self._check(self._lib.gfsm_query_prepare(self._h, query.handle, C.byref(h)))
         return Plan(self, h.value)
 
-    def prepare_queries(self, queries):
+    def plan_for(self, query, data):
+        """A plan whose matching order is chosen for `data` where the count
+        cannot depend on the order (gfsm_query_prepare_for)."""
+        h = C.c_void_p()
+        self._check(self._lib.gfsm_query_prepare_for(self._h, query.handle, data.handle, C.byref(h)))
+        return Plan(self, h.value)
+
+    def prepare_queries(self, queries, data=None):
         """Plans for many queries in one call (gfsm_query_prepare_batch).
 
         queries: iterable of (n, src, dst, elabel or None, vlabel or None),
         directed edge lists with ids local to each query.  The labels must be
-        given for all queries or for none."""
+        given for all queries or for none.  With `data`, each plan is
+        gfsm_query_prepare_for's (data-aware order where it is allowed)."""
         queries = list(queries)
         nq = len(queries)
         if nq == 0:
@@ -236,7 +250,7 @@ class GFSM:
         failed = C.c_int(-1)
         self._check(self._lib.gfsm_query_prepare_batch(
             self._h, nq, nv.ctypes.data_as(_lib.u32p), eoff.ctypes.data_as(_lib.u64p), ptr(src), ptr(dst),
-            ptr(el), ptr(vl), out, C.byref(failed)))
+            ptr(el), ptr(vl), data.handle if data is not None else None, out, C.byref(failed)))
         return [Plan(self, out[i]) for i in range(nq)]
 
     # -- matching -------------------------------------------------------------

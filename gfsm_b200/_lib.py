@@ -30,8 +30,10 @@ SIGNATURES = {
     "gfsm_graph_download": (C.c_int, [vp, vp, u32p, u32p, u8p, u32p]),
     "gfsm_graph_destroy": (None, [vp]),
     "gfsm_query_prepare": (C.c_int, [vp, vp, C.POINTER(vp)]),
-    "gfsm_query_prepare_batch": (C.c_int, [vp, C.c_int, u32p, u64p, u32p, u32p, u32p, u32p, C.POINTER(vp),
+    "gfsm_query_prepare_batch": (C.c_int, [vp, C.c_int, u32p, u64p, u32p, u32p, u32p, u32p, vp, C.POINTER(vp),
                                            C.POINTER(C.c_int)]),
+    "gfsm_query_prepare_for": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
+    "gfsm_plan_info": (C.c_int, [vp, u32p, u32p]),
     "gfsm_plan_tables": (C.c_int, [vp, u32p, u32p, u32p, u32p, u32p]),
     "gfsm_plan_columns": (C.c_int, [vp, u32p]),
     "gfsm_plan_destroy": (None, [vp]),

@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <new>
 #include <thread>
@@ -278,9 +279,100 @@ gfsm_status gfsm_query_prepare(gfsm_ctx *ctx, const gfsm_graph *q, gfsm_plan **o
     return GFSM_OK;
 }
 
+// The data graph's planner statistics, built on first use: vertex labels
+// with their out-degrees, and whether embedding counts are independent of the
+// matching order (every edge has its reverse with the same label and no
+// edge repeats -- what FFS counts with a different anchor edge then equals).
+static const PlanStats &plan_stats(const gfsm_graph *data) {
+    gfsm_graph *g = const_cast<gfsm_graph *>(data);
+    std::lock_guard<std::mutex> lk(g->stats_mu);
+    if (g->stats) return *g->stats;
+    auto st = std::make_unique<PlanStats>();
+    const HostGraph &h = g->h;
+    const uint64_t m = h.src.size();
+    std::vector<uint32_t> outdeg(h.n, 0);
+    for (uint64_t i = 0; i < m; ++i) outdeg[h.src[i]]++;
+    // edges as (src, dst, label) and reversed; equal sorted lists <=> symmetric
+    std::vector<std::pair<uint64_t, uint8_t>> fwd(m), rev(m);
+    for (uint64_t i = 0; i < m; ++i) {
+        fwd[i] = {((uint64_t)h.src[i] << 32) | h.dst[i], h.lab[i]};
+        rev[i] = {((uint64_t)h.dst[i] << 32) | h.src[i], h.lab[i]};
+    }
+    std::sort(fwd.begin(), fwd.end());
+    std::sort(rev.begin(), rev.end());
+    bool inv = fwd == rev;
+    for (uint64_t i = 1; i < m && inv; ++i)
+        if (fwd[i].first == fwd[i - 1].first) inv = false;
+    st->order_invariant = inv;
+    std::vector<uint32_t> lab(h.n, 0);
+    if (g->vl_mode) lab = h.vlabel;
+    st->labels = lab;
+    std::sort(st->labels.begin(), st->labels.end());
+    st->labels.erase(std::unique(st->labels.begin(), st->labels.end()), st->labels.end());
+    st->deg.resize(st->labels.size());
+    for (uint32_t v = 0; v < h.n; ++v) {
+        const size_t li = std::lower_bound(st->labels.begin(), st->labels.end(), lab[v]) - st->labels.begin();
+        st->deg[li].push_back(outdeg[v]);
+    }
+    for (auto &d : st->deg) std::sort(d.begin(), d.end(), std::greater<uint32_t>());
+    g->stats = std::move(st);
+    return *g->stats;
+}
+
+// Data candidates of every query vertex: data vertices with its label (when
+// labels are matched) and, under the degree filter, at least its degree --
+// the sizes of the windows the level steps search.
+static std::vector<double> candidate_weights(const HostGraph &q, const Plan &p, const PlanStats &st, bool vl,
+                                             bool degree_filter) {
+    std::vector<double> w(q.n, 0.0);
+    for (uint32_t d = 0; d < p.k; ++d) {
+        const uint32_t v = p.qvid[d];
+        const uint32_t l = vl ? p.qlabel[d] : 0u;
+        const auto it = std::lower_bound(st.labels.begin(), st.labels.end(), l);
+        if (it == st.labels.end() || *it != l) continue;  // no such label: no candidates
+        const std::vector<uint32_t> &dg = st.deg[it - st.labels.begin()];
+        const uint32_t need = std::max<uint32_t>(degree_filter ? p.qdeg[d] : 0u, 1u);
+        // degrees are descending: count those >= need
+        const size_t c = std::partition_point(dg.begin(), dg.end(), [&](uint32_t x) { return x >= need; }) - dg.begin();
+        w[v] = (double)c;
+    }
+    return w;
+}
+
+// Plans q for data: the data-aware order where the count cannot depend on
+// the order, otherwise the reference's.
+static gfsm_status plan_for(const HostGraph &q, uint32_t rel_bits, const PlanStats *st, const gfsm_limits &lim,
+                            bool vl, Plan &out) {
+    gfsm_status rc = plan_query(q, rel_bits, out);
+    if (rc != GFSM_OK || !st || !st->order_invariant || !out.order_invariant) return rc;
+    const std::vector<double> w = candidate_weights(q, out, *st, vl, lim.degree_filter != 0);
+    Plan alt;
+    if (plan_query(q, rel_bits, alt, &w) == GFSM_OK) out = std::move(alt);
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_query_prepare_for(gfsm_ctx *ctx, const gfsm_graph *q, const gfsm_graph *data, gfsm_plan **out) {
+    if (!ctx || !q || !data || !out) return GFSM_ERR_ARG;
+    *out = nullptr;
+    const PlanStats &st = plan_stats(data);
+    auto p = std::make_unique<gfsm_plan>();
+    gfsm_status rc = plan_for(q->h, q->rel_bits, &st, ctx->lim, data->vl_mode, p->p);
+    if (rc != GFSM_OK) return set_err(ctx, rc, "");
+    *out = p.release();
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_plan_info(const gfsm_plan *p, uint32_t *planner, uint32_t *order_invariant) {
+    if (!p) return GFSM_ERR_ARG;
+    if (planner) *planner = p->p.planner;
+    if (order_invariant) *order_invariant = p->p.order_invariant ? 1u : 0u;
+    return GFSM_OK;
+}
+
 gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, const uint64_t *eoff,
                                      const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
-                                     const uint32_t *vlabel, gfsm_plan **out, int *failed) {
+                                     const uint32_t *vlabel, const gfsm_graph *data, gfsm_plan **out,
+                                     int *failed) {
     if (failed) *failed = -1;
     if (!ctx || nq < 0 || (nq && (!nv || !eoff || !out))) return GFSM_ERR_ARG;
     if (nq == 0) return GFSM_OK;
@@ -292,6 +384,8 @@ gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, 
     std::vector<uint64_t> voff(nq + 1, 0);
     for (int i = 0; i < nq; ++i) voff[i + 1] = voff[i] + nv[i];
     const uint32_t rel_bits = ctx->lim.ccsr_rel_size;
+    const PlanStats *st = data ? &plan_stats(data) : nullptr;
+    const bool vl = data ? data->vl_mode : false;
     std::vector<gfsm_status> rc(nq, GFSM_OK);
     // queries are tiny: one worker per ~64 of them, up to the host's threads
     const int hw = std::max(1u, std::thread::hardware_concurrency());
@@ -305,7 +399,7 @@ gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, 
             if (rc[i] != GFSM_OK) continue;
             auto p = std::unique_ptr<gfsm_plan>(new (std::nothrow) gfsm_plan());
             if (!p) { rc[i] = GFSM_ERR_NOMEM; continue; }
-            rc[i] = plan_query(h, rel_bits, p->p);
+            rc[i] = plan_for(h, rel_bits, st, ctx->lim, vl, p->p);
             if (rc[i] == GFSM_OK) out[i] = p.release();
         }
     };

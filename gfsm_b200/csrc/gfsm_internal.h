@@ -1,6 +1,7 @@
 // gfsm_internal.h -- host/device structures shared inside libgfsm.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -67,6 +68,8 @@ struct Plan {
     std::vector<uint32_t> qlabel;    // depth -> query vertex label value
     std::vector<uint32_t> qdeg;      // depth -> distinct non-self neighbours
     bool symmetric = false;          // query structure is symmetric
+    bool order_invariant = false;    // symmetric with equal labels both ways, no repeated edge
+    uint32_t planner = 0;            // 0: the reference's order; 1: data-aware order
 };
 
 // Per-depth device plan of one query against one data graph.
@@ -132,12 +135,23 @@ struct gfsm_ctx {
     void *engine = nullptr;   // default gfsm::Engine (stream + frontier arena)
 };
 
+namespace gfsm {
+// What the data-aware planner needs of a data graph (built once, on demand).
+struct PlanStats {
+    bool order_invariant = false;            // symmetric with equal labels both ways, no repeated edge
+    std::vector<uint32_t> labels;            // distinct vertex labels, ascending
+    std::vector<std::vector<uint32_t>> deg;  // per label: out-degrees, descending
+};
+}  // namespace gfsm
+
 struct gfsm_graph {
     gfsm_ctx *ctx = nullptr;
     gfsm::HostGraph h;
     gfsm::DeviceGraph *dev = nullptr;
     uint32_t rel_bits = 8;
     bool vl_mode = false;
+    std::mutex stats_mu;
+    std::unique_ptr<gfsm::PlanStats> stats;
 };
 
 struct gfsm_plan {
@@ -148,7 +162,10 @@ namespace gfsm {
 // host_graph.cpp
 gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGraph &g);
 gfsm_status read_file(const char *path, std::string &out);
-gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p);
+// weight == nullptr: the reference's matching order.  Otherwise weight[v]
+// estimates query vertex v's data candidates and the order is data-aware
+// (only valid where the count cannot depend on the order).
+gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std::vector<double> *weight = nullptr);
 // builder.cu
 gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, DeviceGraph &out,
                                std::string &err);

@@ -183,7 +183,7 @@ gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGra
 // ---------------------------------------------------------------------------
 // Planner
 // ---------------------------------------------------------------------------
-gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p) {
+gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std::vector<double> *weight) {
     p = Plan();
     p.rel_bits = rel_bits;
     const uint32_t k = q.n;
@@ -217,19 +217,60 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p) {
     p.header.assign(3 * (size_t)k, 0);
     p.reqs.assign(2 * (size_t)maxv * k, 0);
     std::vector<int32_t> mapping(k, -1);
-    mapping[0] = 0;  // HnGPU.cu:759-769: the first row has the maximal degree
+    // mapping[r]: -1 unseen, 0 seen (a neighbour of a placed row), d + 1 for
+    // a row placed d depths ago.
+    if (!weight) {
+        mapping[0] = 0;  // HnGPU.cu:759-769: the first row has the maximal degree
+    } else {
+        // data-aware root: fewest data candidates per query edge
+        uint32_t best = 0;
+        double best_c = 0.0;
+        for (uint32_t r = 0; r < k; ++r) {
+            const double c = (*weight)[rowvid[r]] / (double)rows[r].size();
+            if (r == 0 || c < best_c) { best = r; best_c = c; }
+        }
+        mapping[best] = 0;
+    }
     for (uint32_t depth = 0; depth < k; ++depth) {  // HnGPU.cu:771-773
-        // ccsr.cpp:114-123
         uint32_t rel_depth = 0;
         bool found = false;
-        for (uint32_t i = 0; i < k; ++i) {
-            if (mapping[i] == 0 && !found) {
-                mapping[i] = 1;
-                rel_depth = i;
-                found = true;
-            } else if (mapping[i] > 0) {
-                mapping[i]++;
+        if (!weight) {
+            // ccsr.cpp:114-123: the first seen row in CCSR row order
+            for (uint32_t i = 0; i < k; ++i) {
+                if (mapping[i] == 0 && !found) {
+                    mapping[i] = 1;
+                    rel_depth = i;
+                    found = true;
+                } else if (mapping[i] > 0) {
+                    mapping[i]++;
+                }
             }
+        } else {
+            // data-aware: the seen row with the most placed neighbours (each
+            // one a requirement that prunes), then the fewest data candidates
+            uint32_t best_back = 0;
+            double best_c = 0.0;
+            for (uint32_t i = 0; i < k; ++i) {
+                if (mapping[i] != 0) continue;
+                uint32_t back = 0, last = ~0u;
+                for (auto &ent : rows[i])
+                    if (ent.first != last) {
+                        last = ent.first;
+                        back += mapping[ent.first] > 0 ? 1u : 0u;
+                    }
+                const double c = (*weight)[rowvid[i]];
+                if (!found || back > best_back || (back == best_back && c < best_c)) {
+                    rel_depth = i;
+                    best_back = back;
+                    best_c = c;
+                    found = true;
+                }
+            }
+            if (found)
+                for (uint32_t i = 0; i < k; ++i) {
+                    if (i == rel_depth) mapping[i] = 1;
+                    else if (mapping[i] > 0) mapping[i]++;
+                }
         }
         if (!found) return GFSM_ERR_QUERY;  // ccsr.cpp:126-128
         p.order[depth] = rel_depth;
@@ -295,6 +336,20 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p) {
             if (!back) { sym = false; break; }
         }
     p.symmetric = sym;
+    // every entry has its reverse with the same label, and no (row, target)
+    // pair repeats: a count that cannot depend on the matching order
+    bool inv = sym;
+    for (uint32_t u = 0; u < k && inv; ++u)
+        for (size_t i = 0; i < rows[u].size() && inv; ++i) {
+            const auto &ent = rows[u][i];
+            if (i && rows[u][i - 1].first == ent.first) { inv = false; break; }
+            bool back = false;
+            for (auto &b : rows[ent.first])
+                if (b.first == u && b.second == ent.second) { back = true; break; }
+            inv = back;
+        }
+    p.order_invariant = inv;
+    p.planner = weight ? 1 : 0;
     return GFSM_OK;
 }
 

@@ -142,18 +142,33 @@ void        gfsm_graph_destroy(gfsm_graph *g);
  * CCSR::genereateCCSRRequirements (ccsr.cpp:98-204): the reference's
  * matching order and requirement table. */
 gfsm_status gfsm_query_prepare(gfsm_ctx *ctx, const gfsm_graph *query, gfsm_plan **out);
-/* gfsm_graph_from_edges + gfsm_query_prepare for nq queries in one call,
- * spread over the host's threads.  No counterpart in the reference, which
- * plans one query per process (main.cu:56-65); for the batched and served
- * forms.  Query i has nv[i] vertices and the directed edges
- * [eoff[i], eoff[i+1]) of src/dst/elabel (ids local to the query); its
- * vertex labels are the next nv[i] entries of vlabel (query after query).
- * elabel / vlabel may be NULL.  On success out[i] is query i's plan; on
- * failure every out[i] is NULL, *failed (if given) is the first failing
- * query and that query's status is returned. */
+/* Plans a query for one data graph: where the embedding count cannot depend
+ * on the matching order (query and data symmetric with equal labels both
+ * ways, no repeated edge), a data-aware order -- root with the fewest data
+ * candidates per query edge, then the seen vertex with the most placed
+ * neighbours, then the fewest candidates; otherwise the reference's order.
+ * No counterpart in the reference (its order is fixed, ccsr.cpp:114-123).
+ * The plan counts the same embeddings; matching it against another data
+ * graph is allowed but may be slower. */
+gfsm_status gfsm_query_prepare_for(gfsm_ctx *ctx, const gfsm_graph *query, const gfsm_graph *data,
+                                   gfsm_plan **out);
+/* planner: 0 the reference's order, 1 data-aware; order_invariant: 1 if the
+ * query's count cannot depend on the order.  Either pointer may be NULL. */
+gfsm_status gfsm_plan_info(const gfsm_plan *p, uint32_t *planner, uint32_t *order_invariant);
+/* gfsm_graph_from_edges + gfsm_query_prepare (data == NULL) or
+ * gfsm_query_prepare_for (data given) for nq queries in one call, spread
+ * over the host's threads.  No counterpart in the reference, which plans one
+ * query per process (main.cu:56-65); for the batched and served forms.
+ * Query i has nv[i] vertices and the directed edges [eoff[i], eoff[i+1]) of
+ * src/dst/elabel (ids local to the query); its vertex labels are the next
+ * nv[i] entries of vlabel (query after query).  elabel / vlabel may be NULL.
+ * On success out[i] is query i's plan; on failure every out[i] is NULL,
+ * *failed (if given) is the first failing query and that query's status is
+ * returned. */
 gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, const uint64_t *eoff,
                                      const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
-                                     const uint32_t *vlabel, gfsm_plan **out, int *failed);
+                                     const uint32_t *vlabel, const gfsm_graph *data, gfsm_plan **out,
+                                     int *failed);
 /* The plan in the reference's buffer layout: order[k] (query row index per
  * depth), header[3k] {numReqs, reqOffset, firstQ}, reqs[2*maxValency*k]
  * {distance delta, relation bits}.  Any output pointer may be NULL. */

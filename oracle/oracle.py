@@ -141,6 +141,20 @@ class Plan:
             pass
 
 
+class TablePlan:
+    """A plan given as tables (order, header, reqs in the reference's packed
+    layout), e.g. one made with another matching order; ffs_count runs the
+    same level semantics over it."""
+
+    def __init__(self, q, tables, rel_bits=8):
+        self._keep = [np.ascontiguousarray(tables[k], np.uint32) for k in ("reqs", "header", "order")]
+        reqs, header, order = self._keep
+        self._p = OrcPlan(k=int(tables["k"]), max_valency=int(tables["max_valency"]), rel_bits=rel_bits,
+                          reqs=reqs.ctypes.data_as(u32p), header=header.ctypes.data_as(u32p),
+                          order=order.ctypes.data_as(u32p), err=0)
+        self.q = q
+
+
 def ffs_count(q, plan, d, vlabel_mode=False, threads=1, max_rows=0):
     """Reference-semantics count; with max_rows, also the mappings (ids)."""
     cnt = C.c_uint64()

@@ -385,3 +385,56 @@ def test_shared_prefix_batches(monkeypatch):
     assert st1["candidates"] < st0["candidates"]  # levels 0 and 1 ran once per class
     assert sum(single) > 0
     ctx.close()
+
+
+@pytest.mark.parametrize("gen", range(len(GENS)))
+def test_data_aware_order(gpu_ctx_vl, tmp_path, gen):
+    """Plans with the data-aware matching order (gfsm_query_prepare_for, Zipf
+    vertex labels so label windows differ) count exactly what the reference
+    order counts -- on the device, and in the oracle run over the same plan
+    tables; the batch planner with a data graph gives the same plans."""
+    name, fn = GENS[gen]
+    g = fn(gen + 11)
+    g.vlabel = synth.vlabels(g.n, 5, 1.0, seed=gen + 60)
+    dpath = tmp_path / "d.g"
+    g.write_text(str(dpath))
+    od = O.Graph(path=str(dpath))
+    ds, dd = g.directed()
+    data = gpu_ctx_vl.graph_from_edges(g.n, ds, dd, None, g.vlabel)
+    qd, differ = [], 0
+    for i, k in enumerate((3, 4, 5, 6, 7, 5, 6, 7)):
+        qg, _ = synth.rw_query(g, k, tree=i % 3 == 1, seed=700 * gen + i)
+        qpath = tmp_path / "q.g"
+        qg.write_text(str(qpath))
+        q = gpu_ctx_vl.file_parse(str(qpath))
+        ref, mine = gpu_ctx_vl.pre_process_query(q), gpu_ctx_vl.plan_for(q, data)
+        assert mine.info() == {"planner": 1, "order_invariant": True}
+        oq = O.Graph(path=str(qpath))
+        expect = O.ffs_count(oq, O.Plan(oq), od, vlabel_mode=True, threads=8)
+        assert O.ffs_count(oq, O.TablePlan(oq, mine.tables()), od, vlabel_mode=True, threads=8) == expect
+        assert gpu_ctx_vl.match_count(ref, data)[0] == expect
+        assert gpu_ctx_vl.match_count(mine, data)[0] == expect, (name, k, i)
+        differ += mine.tables()["order"].tolist() != ref.tables()["order"].tolist()
+        qs, qt = qg.directed()
+        qd.append((qg.n, qs, qt, None, qg.vlabel))
+    assert differ > 0
+    batch = gpu_ctx_vl.prepare_queries(qd, data)
+    singles = [gpu_ctx_vl.plan_for(gpu_ctx_vl.graph_from_edges(*q), data) for q in qd]
+    for a, b in zip(batch, singles):
+        assert a.tables()["order"].tolist() == b.tables()["order"].tolist()
+    c1, _ = gpu_ctx_vl.batch_count(batch, data)
+    c2, _ = gpu_ctx_vl.batch_count(gpu_ctx_vl.prepare_queries(qd), data)
+    assert c1.tolist() == c2.tolist()
+
+
+def test_data_aware_order_falls_back_on_directed_data(gpu_ctx):
+    """Where the count could depend on the order (a data edge without its
+    reverse), gfsm_query_prepare_for keeps the reference's order."""
+    g = synth.er(200, 4.0, seed=9)
+    s, d = g.src.astype(np.uint32), g.dst.astype(np.uint32)   # one direction only
+    data = gpu_ctx.graph_from_edges(g.n, s, d)
+    q = gpu_ctx.file_parse(_g("queries/_3_triangle"))
+    mine, ref = gpu_ctx.plan_for(q, data), gpu_ctx.pre_process_query(q)
+    assert mine.info()["planner"] == 0
+    assert mine.tables()["order"].tolist() == ref.tables()["order"].tolist()
+    assert gpu_ctx.match_count(mine, data)[0] == gpu_ctx.match_count(ref, data)[0]

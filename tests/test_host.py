@@ -163,7 +163,7 @@ def test_batch_planning_reports_the_failing_query(host_ctx):
     failed = C.c_int(7)
     rc = lib.gfsm_query_prepare_batch(host_ctx._h, 2, nv.ctypes.data_as(_lib.u32p), eoff.ctypes.data_as(_lib.u64p),
                                       src.ctypes.data_as(_lib.u32p), dst.ctypes.data_as(_lib.u32p), None, None,
-                                      out, C.byref(failed))
+                                      None, out, C.byref(failed))
     assert rc == 1 and failed.value == 1 and out[0] is None and out[1] is None
     bad = (3, [0, 1, 5], [1, 0, 0], None, None)
     with pytest.raises(gfsm_b200.GFSMError) as ei:

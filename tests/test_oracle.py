@@ -180,3 +180,40 @@ def test_reference_frontend_live(tmp_path):
         assert rc == 0
         assert r["segments"].tolist() == REF["queries/" + name]["segments"]
         assert r["reqs"].tolist() == REF["queries/" + name]["reqs"]
+
+
+@pytest.mark.parametrize("vl", [False, True])
+def test_data_aware_order_counts_the_same(tmp_path, vl):
+    """Plans from gfsm_query_prepare_for (data-aware matching order), run by
+    the oracle's level semantics, count what the reference order counts and
+    what the independent backtracking enumerator counts."""
+    import gfsm_b200
+    from gfsm_b200 import synth
+    ctx = gfsm_b200.GFSM(device=-1, vertex_labels=int(vl))
+    gens = [synth.er(300, 5, seed=3), synth.ba(300, 2, seed=4), synth.grid(16, 0.05, 0.02, seed=5)]
+    differ = 0
+    for gi, g in enumerate(gens):
+        g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=6 + gi)
+        dpath = tmp_path / f"d{gi}.g"
+        g.write_text(str(dpath))
+        data = ctx.file_parse(str(dpath))
+        od = O.Graph(path=str(dpath))
+        for i in range(12):
+            k = 3 + i % 4 if not vl else 3 + i % 5
+            qg, _ = synth.rw_query(g, k, tree=i % 3 == 0, seed=50 * gi + i)
+            qpath = tmp_path / f"q{gi}_{i}.g"
+            qg.write_text(str(qpath))
+            q = ctx.file_parse(str(qpath))
+            mine = ctx.plan_for(q, data)
+            ref = ctx.pre_process_query(q)
+            assert mine.info()["order_invariant"]
+            oq = O.Graph(path=str(qpath))
+            c_ref = O.ffs_count(oq, O.Plan(oq), od, vlabel_mode=vl)
+            c_mine = O.ffs_count(oq, O.TablePlan(oq, mine.tables()), od, vlabel_mode=vl)
+            qs, qd = qg.directed()
+            ds, dd = g.directed()
+            c_bt = O.bt_count(qg.n, qs, qd, None, qg.vlabel, g.n, ds, dd, None, g.vlabel, vlabel_mode=vl)
+            assert c_mine == c_ref == c_bt, (gi, i, c_mine, c_ref, c_bt)
+            differ += mine.tables()["order"].tolist() != ref.tables()["order"].tolist()
+    if vl:  # unlabelled, both orders take high-degree rows first and mostly agree
+        assert differ > 0
