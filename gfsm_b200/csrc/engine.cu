@@ -86,9 +86,9 @@ __device__ __forceinline__ uint32_t row_lower_bound(const uint32_t *__restrict__
     return n <= SHORT_ROW ? short_lower_bound(a, n, key) : lower_bound_u32(a, n, key);
 }
 
-// reqExists (HnGPU.cu:34-52) as a search: does u's row hold (v, lab)?
-__device__ __forceinline__ bool has_edge(const GraphView &g, uint32_t u, uint32_t v, uint32_t lab) {
-    const uint32_t rs = __ldg(g.rowptr + u), re = __ldg(g.rowptr + u + 1);
+// reqExists (HnGPU.cu:34-52) as a search: does the row adj[rs, re) hold
+// (v, lab)?
+__device__ __forceinline__ bool row_holds(const GraphView &g, uint32_t rs, uint32_t re, uint32_t v, uint32_t lab) {
     if (!g.elab && lab != g.single_label) return false;
     if (!g.elab && re - rs <= SHORT_ROW) {
         bool f = false;
@@ -102,6 +102,11 @@ __device__ __forceinline__ bool has_edge(const GraphView &g, uint32_t u, uint32_
     for (; p < re && __ldg(g.adj + p) == v; ++p)
         if (__ldg(g.elab + p) == lab) return true;
     return false;
+}
+
+// Does u's row hold (v, lab)?
+__device__ __forceinline__ bool has_edge(const GraphView &g, uint32_t u, uint32_t v, uint32_t lab) {
+    return row_holds(g, __ldg(g.rowptr + u), __ldg(g.rowptr + u + 1), v, lab);
 }
 
 struct StepArgs {
@@ -345,37 +350,36 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
         // injectivity (HnGPU.cu:223-236)
         for (uint32_t i = 0; i < d; ++i)
             if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
-        if (local == 0) {
-            // algorithmic bytes of this parent: its tuple and every backward
-            // neighbour's row (anchor + requirement rows), read once
-            const uint32_t anchor = __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p);
-            unsigned long long b = 4ull * d;
-            b += 4ull * (__ldg(a.g.rowptr + anchor + 1) - __ldg(a.g.rowptr + anchor) + 1);
-            for (uint32_t r = 0; r < L->nreq; ++r) {
-                const uint32_t pos = L->req_pos[r];
-                if (pos == REQ_SELF) continue;
-                const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                b += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
-            }
-            my_bytes += b;
-        }
     }
+    // Algorithmic bytes of a parent (its tuple, its anchor row and every
+    // requirement row, each read once): the tuple and anchor-row terms were
+    // added when the parent was written (below, where the anchor row's bounds
+    // are at hand); the parent's first candidate adds its requirement rows
+    // here, from the same row bounds the requirement checks load.
+    const bool acct = !ROOT && local == 0;
     // remaining requirements (HnGPU.cu:243-252)
-    for (uint32_t r = 0; r < L->nreq && pass; ++r) {
+    for (uint32_t r = 0; r < L->nreq && (pass || acct); ++r) {
         const uint32_t mode = (t.single && r < (uint32_t)NSTAGE) ? t.rmode[r] : 0u;
+        const uint32_t pos = L->req_pos[r];
+        if (mode == 0u) {
+            const uint32_t u = pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+            const uint32_t rs = __ldg(a.g.rowptr + u), re = __ldg(a.g.rowptr + u + 1);
+            if (acct && pos != REQ_SELF) my_bytes += 4ull * (re - rs + 1);
+            if (pass) pass = row_holds(a.g, rs, re, v, L->req_lab[r]);
+            continue;
+        }
+        if (acct) {  // a staged row (pos is never REQ_SELF there)
+            const uint32_t u = __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+            my_bytes += 4ull * (__ldg(a.g.rowptr + u + 1) - __ldg(a.g.rowptr + u) + 1);
+        }
+        if (!pass) continue;
+        const uint32_t n = t.rhi[r] - t.rlo[r];
         if (mode == 1u) {
-            const uint32_t n = t.rhi[r] - t.rlo[r];
             const uint32_t k = smem_lower_bound(t.req + r * t.req_stride, n, v);
             pass = k < n && t.req[r * t.req_stride + k] == v && L->req_lab[r] == a.g.single_label;
-        } else if (mode == 2u) {
-            const uint32_t n = t.rhi[r] - t.rlo[r];
+        } else {
             const uint32_t k = lower_bound_u32(a.g.adj + t.rlo[r], n, v);
             pass = k < n && __ldg(a.g.adj + t.rlo[r] + k) == v && L->req_lab[r] == a.g.single_label;
-        } else {
-            const uint32_t pos = L->req_pos[r];
-            const uint32_t u =
-                pos == REQ_SELF ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-            pass = has_edge(a.g, u, v, L->req_lab[r]);
         }
     }
     if (pass) {
@@ -408,8 +412,10 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             if (e > s) {  // a child with no candidates cannot be extended: not written
                 emit = true;
                 // a shared class's child offers its slice to every member
-                const uint32_t cnt = L->fanout_next ? (e - s) * __ldg(a.csize + q) : e - s;
-                rec = Stage{p, v, s, cnt, q};
+                const uint32_t mult = L->fanout_next ? __ldg(a.csize + q) : 1u;
+                rec = Stage{p, v, s, (e - s) * mult, q};
+                // the child's tuple and anchor row, read once per (member) parent
+                my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
             }
         }
     }
