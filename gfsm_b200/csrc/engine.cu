@@ -72,18 +72,19 @@ struct GraphView {
 // searched in registers instead of by a chain of dependent probes.
 constexpr uint32_t SHORT_ROW = 8;
 
-// First index in the row a[0, n) with a[i] >= key, n <= SHORT_ROW.
-__device__ __forceinline__ uint32_t short_lower_bound(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
-    uint32_t r = 0;
+// Entries of the row a[0, n), n <= SHORT_ROW, below k1 and below k2: one
+// pass, the loads independent of each other.
+__device__ __forceinline__ void short_bounds(const uint32_t *__restrict__ a, uint32_t n, uint32_t k1, uint32_t k2,
+                                             uint32_t &r1, uint32_t &r2) {
+    r1 = 0;
+    r2 = 0;
 #pragma unroll
     for (uint32_t i = 0; i < SHORT_ROW; ++i)
-        if (i < n && __ldg(a + i) < key) ++r;
-    return r;
-}
-
-// First index in a[0, n) whose value is >= key, for any n.
-__device__ __forceinline__ uint32_t row_lower_bound(const uint32_t *__restrict__ a, uint32_t n, uint32_t key) {
-    return n <= SHORT_ROW ? short_lower_bound(a, n, key) : lower_bound_u32(a, n, key);
+        if (i < n) {
+            const uint32_t x = __ldg(a + i);
+            r1 += x < k1;
+            r2 += x < k2;
+        }
 }
 
 // reqExists (HnGPU.cu:34-52) as a search: does the row adj[rs, re) hold
@@ -406,9 +407,16 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             const uint32_t na = L->next_anchor;
             const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
             const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-            const uint32_t s = L->next_lo ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_lo) : rs;
-            const uint32_t e =
-                L->next_hi < a.g.n ? rs + row_lower_bound(a.g.adj + rs, re - rs, L->next_hi) : re;
+            uint32_t s = rs, e = re;  // the part of w's row inside depth+1's window
+            if (re - rs <= SHORT_ROW) {
+                uint32_t b1, b2;
+                short_bounds(a.g.adj + rs, re - rs, L->next_lo, L->next_hi, b1, b2);
+                s = rs + b1;
+                e = rs + b2;
+            } else {
+                if (L->next_lo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo);
+                if (L->next_hi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi);
+            }
             if (e > s) {  // a child with no candidates cannot be extended: not written
                 emit = true;
                 // a shared class's child offers its slice to every member
