@@ -8,6 +8,10 @@
 // environment variables.  GFSM_OUTPUT=1 also writes the mappings to
 // output.fs in the reference's binary layout (HnGPU.cu:1081-1091:
 // u32 count, u32 width, u32[count*width]), columns = query vertex ids.
+// GFSM_PLANNER=data plans the query for the data graph (data-aware matching
+// order where the count cannot depend on the order); the default is the
+// reference's order.
+#include <cstring>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -55,7 +59,9 @@ int run(const std::string &qpath, const std::string &dpath) {
 
     auto solve0 = Clock::now();
     gfsm_plan *plan = nullptr;
-    rc = gfsm_query_prepare(ctx, q, &plan);
+    const char *planner = getenv("GFSM_PLANNER");
+    rc = planner && !strcmp(planner, "data") ? gfsm_query_prepare_for(ctx, q, d, &plan)
+                                             : gfsm_query_prepare(ctx, q, &plan);
     if (rc != GFSM_OK) return fail(ctx, rc);
     uint64_t count = 0;
     gfsm_stats st{};

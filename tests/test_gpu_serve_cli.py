@@ -117,3 +117,30 @@ def test_cli_output_fs(tmp_path):
     for row in rows[:5000]:
         for a, b in zip(qs, qd):
             assert (int(row[a]), int(row[b])) in dset
+
+
+def test_cli_data_aware_planner(tmp_path):
+    """GFSM_PLANNER=data (vertex labels matched, Zipf-distributed so the
+    data-aware order differs from the reference's): same count and, with
+    GFSM_OUTPUT, the same mapping set (columns stay query vertex ids)."""
+    from gfsm_b200 import synth
+    g = synth.er(400, 5.0, seed=21)
+    g.vlabel = synth.vlabels(g.n, 5, 1.0, seed=22)
+    d = str(tmp_path / "d.g")
+    g.write_text(d)
+    qg, _ = synth.rw_query(g, 5, seed=8)
+    q = str(tmp_path / "q.g")
+    qg.write_text(q)
+    counts, sets = [], []
+    for env in ({}, {"GFSM_PLANNER": "data"}):
+        sub = tmp_path / ("data" if env else "ref")
+        sub.mkdir()
+        r = _run([q, d], env=dict(env, GFSM_OUTPUT="1", GFSM_VERTEX_LABELS="1"), cwd=str(sub))
+        assert r.returncode == 0, r.stderr
+        counts.append(int(r.stdout.strip().split("\n")[-1].rstrip(",").split(",")[8]))
+        w = np.fromfile(sub / "output.fs", np.uint32)
+        rows = w[2:].reshape(int(w[0]), int(w[1]))
+        sets.append(rows[np.lexsort(rows.T[::-1])])
+    oq, od = O.Graph(path=q), O.Graph(path=d)
+    assert counts[0] == counts[1] == O.ffs_count(oq, O.Plan(oq), od, vlabel_mode=True) > 0
+    assert np.array_equal(sets[0], sets[1])
