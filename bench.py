@@ -40,6 +40,13 @@ KMIN, KMAX = 4, 10
 SERVE_RATES = (100, 1000, 10000)
 WORKLOAD = ("config5 road-like grid 1400x1400 (5% edges removed, 2% shortcuts, 4 uniform vertex labels, "
             "vertex labels matched), 4096 random-walk queries of 4-10 vertices with all induced edges")
+METRIC = "queries/s (batched, exact counts) with p99 latency; plain and served beside it"
+
+
+def config_for(queries, world):
+    """The workload description both arms print."""
+    return {"workload": WORKLOAD, "queries_per_step": queries, "vertex_labels": True,
+            "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}"}
 
 
 def parse_args():
@@ -228,10 +235,10 @@ def run_reference(args, rank, world, pg):
     el = sum(e for _, e in per_step)
     qps = total_q / el if el else 0.0
     line = {
-        "impl": "reference", "metric": "queries/s (batched, exact counts)", "value": qps, "unit": "queries/s",
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / len(per_step),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "queries_per_step": args.queries},
+        "config": config_for(args.queries, args.gpus),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
                          "sample": f"first queries of the batch, ~8 s of CPU per step ({total_q} queries timed)"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -410,12 +417,11 @@ def run_ours(args, rank, world, local, pg):
 
     if rank == 0:
         line = {
-            "metric": "queries/s (batched, exact counts) with p99 latency; plain and served beside it",
+            "metric": METRIC,
             "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "queries_per_step": args.queries, "vertex_labels": True,
-                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}"},
+            "config": config_for(args.queries, world),
             "exact": exact, "batched_over_plain": value / plain["queries_per_s"] if plain else None,
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
