@@ -245,6 +245,11 @@ using Geo0 = Geo<256, 4, 6>;   // 1024-candidate tiles, 8 warps (the default)
 using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
 using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
 using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
+// Survivors one warp stages per tile, at most; their slice counts are
+// summed in 32 bits (see the class-size cap in Engine::run).
+constexpr uint64_t kWarpStage = 128;
+static_assert(Geo0::WC <= kWarpStage && Geo1::WC <= kWarpStage && Geo2::WC <= kWarpStage && Geo3::WC <= kWarpStage,
+              "a warp stages at most kWarpStage survivors");
 constexpr int kVariants = 4;
 constexpr uint32_t kMinTile = 512;   // the tile directory is sized for this tile
 __host__ __device__ constexpr uint32_t variant_tile(int v) {
@@ -1156,14 +1161,24 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<uint32_t> csize(na, 1), mstart(na, 0), members, root_lo, root_hi;
     std::vector<std::vector<uint32_t>> cls_members;
     uint32_t root_base = 0;
+    // A tuple's next-level candidate count (its row slice, times its class's
+    // size) and a warp's running sum of up to kWarpStage of them are 32-bit:
+    // the data graph's largest row bounds both, and caps a class's size.
+    const uint64_t row_max = std::max<uint64_t>(g.max_degree, 1);
+    if (row_max * kWarpStage > 0xffffffffull) {
+        err = "a data row of " + std::to_string(g.max_degree) + " entries exceeds the level step's 32-bit slice sums";
+        return GFSM_ERR_TOO_LARGE;
+    }
+    const uint64_t class_cap = 0xffffffffull / (row_max * kWarpStage);
     if (share) {
-        std::map<std::string, uint32_t> cls;
+        std::map<std::string, uint32_t> cls;  // prefix -> its class that still has room
         for (uint32_t i = 0; i < na; ++i) {
             const std::string key(reinterpret_cast<const char *>(&dq[i].lv[0]), 2 * sizeof(DLevel));
             auto it = cls.find(key);
-            if (it == cls.end()) {
-                it = cls.emplace(key, (uint32_t)cls_members.size()).first;
+            if (it == cls.end() || cls_members[it->second].size() >= class_cap) {
+                cls[key] = (uint32_t)cls_members.size();
                 cls_members.emplace_back();
+                it = cls.find(key);
             }
             cls_members[it->second].push_back(i);
         }

@@ -438,3 +438,27 @@ def test_data_aware_order_falls_back_on_directed_data(gpu_ctx):
     assert mine.info()["planner"] == 0
     assert mine.tables()["order"].tolist() == ref.tables()["order"].tolist()
     assert gpu_ctx.match_count(mine, data)[0] == gpu_ctx.match_count(ref, data)[0]
+
+
+def test_shared_class_split_by_row_size():
+    """A class's size times the largest data row must fit the level step's
+    32-bit slice sums: a 40,000-entry row caps classes at 838 members, so 900
+    identical triangle queries form two classes -- every count still equals
+    the single-query count (60: the ordered triangles of a K5)."""
+    ctx = gfsm_b200.GFSM(device=0)
+    m = 40000
+    src = list(np.zeros(m, np.uint32)) + list(range(1, m + 1))
+    dst = list(range(1, m + 1)) + list(np.zeros(m, np.uint32))
+    k5 = [m + 1 + i for i in range(5)]
+    for a in k5:
+        for b in k5:
+            if a != b:
+                src.append(a)
+                dst.append(b)
+    data = ctx.graph_from_edges(m + 6, np.array(src, np.uint32), np.array(dst, np.uint32))
+    tri = ctx.pre_process_query(ctx.file_parse(_g("queries/_3_triangle")))
+    one = ctx.match_count(tri, data)[0]
+    assert one == 60
+    counts, st = ctx.batch_count([tri] * 900, data)
+    assert counts.tolist() == [one] * 900
+    ctx.close()
