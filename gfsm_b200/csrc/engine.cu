@@ -136,15 +136,14 @@ struct StepArgs {
     uint32_t *rows_out;
     uint64_t max_rows;
     uint32_t *rows_ctr;
-    // shared query prefixes: root parents are entities root_base + i; a class
-    // entity stands for csize[e] member queries members[mstart[e] ..]; the
-    // fan-out step maps each candidate to (member, row offset)
-    uint32_t root_base;
-    uint32_t fanout;
-    const uint32_t *__restrict__ csize;
-    const uint32_t *__restrict__ mstart;
-    const uint32_t *__restrict__ members;
+    // shared query prefixes: root parent i is the trie node of query
+    // root_rep[i]; a tuple's query id is its node's representative, with
+    // kBranch set when the node has several child nodes (fan_list)
+    const uint32_t *__restrict__ root_rep;
+    const uint32_t *__restrict__ fan_list;
 };
+
+constexpr uint32_t kBranch = 1u << 31;
 
 // Also zeroes the step's per-query count scratch: final-level counts of a
 // step are added to the totals only once the host accepts the step, so a step
@@ -330,15 +329,17 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
     const uint32_t p = t.plo + lo;
     const unsigned long long pc = t.win ? t.win[lo] : __ldg(a.pcoff + p);
     uint32_t local = (uint32_t)(c - pc);
-    uint32_t q = ROOT ? a.root_base + p : __ldg(a.ptup + p);
-    if (!ROOT && a.fanout) {
-        // a shared class tuple: candidates run over (member, row offset)
-        const uint32_t size = __ldg(a.csize + q);
+    uint32_t q = ROOT ? __ldg(a.root_rep + p) : __ldg(a.ptup + p);
+    if (!ROOT && (q & kBranch)) {
+        // the parent's trie node branches: its candidates run over (child
+        // node, row offset), one copy of its slice per child node
+        q &= ~kBranch;
+        const DLevel *P = &a.plans[q].lv[d - 1];
         const unsigned long long pn = t.win ? t.win[lo + 1] : __ldg(a.pcoff + p + 1);
-        const uint32_t slen = (uint32_t)((pn - pc) / size);
+        const uint32_t slen = (uint32_t)((pn - pc) / P->fan_count);
         const uint32_t j = local / slen;
         local -= j * slen;
-        q = __ldg(a.members + __ldg(a.mstart + q) + j);
+        q = __ldg(a.fan_list + P->fan_start + j);
     }
     const DLevel *L = &a.plans[q].lv[d];
     uint32_t v;
@@ -424,9 +425,10 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             }
             if (e > s) {  // a child with no candidates cannot be extended: not written
                 emit = true;
-                // a shared class's child offers its slice to every member
-                const uint32_t mult = L->fanout_next ? __ldg(a.csize + q) : 1u;
-                rec = Stage{p, v, s, (e - s) * mult, q};
+                // a branching node's child offers its slice to every child node
+                const uint32_t nf = L->fan_count;
+                const uint32_t mult = nf > 1 ? nf : 1u;
+                rec = Stage{p, v, s, (e - s) * mult, nf > 1 ? (q | kBranch) : q};
                 // the child's tuple and anchor row, read once per (member) parent
                 my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
             }
@@ -454,7 +456,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
 
     // ---- a tile inside one parent's slice (hub rows): stage the part of each
     // requirement row that can hold this tile's candidates
-    const bool single = !ROOT && plo == phi && a.g.elab == nullptr && !a.fanout;
+    const bool single = !ROOT && plo == phi && a.g.elab == nullptr && !(__ldg(a.ptup + plo) & kBranch);
     if (single) {
         const uint32_t q0 = __ldg(a.ptup + plo);
         const DLevel *L0 = &a.plans[q0].lv[d];
@@ -486,7 +488,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
         }
     }
-    if (tid == 0) sm.q0 = ROOT ? a.root_base + plo : __ldg(a.ptup + plo);
+    if (tid == 0) sm.q0 = ROOT ? __ldg(a.root_rep + plo) : (__ldg(a.ptup + plo) & ~kBranch);
     __syncthreads();
 
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
@@ -643,7 +645,7 @@ struct Ctl {
     const unsigned long long *root_coff;
     const uint32_t *root_cstart;
     unsigned long long *counts;        // per-entity totals (args.counts is the step scratch)
-    uint32_t nq, accepted, share_depth;
+    uint32_t nq, accepted;
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
     uint32_t d, dmax, emits, done, err;
@@ -700,7 +702,6 @@ __device__ void ctl_plan(Ctl &c) {
         a.ccstart = nullptr;
         a.ccoff = nullptr;
     }
-    a.fanout = c.share_depth && d == c.share_depth;
     c.chunk = chunk;
     c.emits = emits;
     *a.tile_ctr = 0;
@@ -1150,64 +1151,88 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     const uint64_t rows_bytes = rows_out ? max_rows * (uint64_t)dq[0].k * 4 : 0;
 
-    // Shared prefixes: queries whose device plans for depths 0 and 1 are
-    // byte-identical (windows, requirements, final flags and the depth-2
-    // slice) form a class; depths 0 and 1 run once per class and the depth-2
-    // step fans each class tuple out to its members.  Entities are the
-    // queries [0, na) followed by the classes [na, na + ncls).
+    // Shared prefixes: a trie of the queries' device plans.  A node at depth
+    // d is a set of queries whose plans for depths 0..d are byte-identical
+    // (windows, requirements, final flags and the depth-(d+1) slice), so one
+    // tuple stands for all of them.  A node is named by its smallest member
+    // (its representative); a node with several child nodes lists their
+    // representatives in fan_list, recorded in the representative's lv[d]
+    // (fan_start, fan_count), and the step at depth d+1 runs such a parent's
+    // candidates over (child node, row offset).  Final-level counts go to the
+    // final node's representative and are copied to its members here.
     const char *shr = getenv("GFSM_SHARE");
-    const bool share = !rows_out && na >= 2 && dmax >= 2 && !(shr && *shr == '0');
-    std::vector<DQuery> ent(dq);
-    std::vector<uint32_t> csize(na, 1), mstart(na, 0), members, root_lo, root_hi;
-    std::vector<std::vector<uint32_t>> cls_members;
-    uint32_t root_base = 0;
-    // A tuple's next-level candidate count (its row slice, times its class's
-    // size) and a warp's running sum of up to kWarpStage of them are 32-bit:
-    // the data graph's largest row bounds both, and caps a class's size.
+    bool share = !rows_out && na >= 2 && !(shr && *shr == '0');
+    // A tuple's next-level candidate count (its row slice, times its node's
+    // child nodes) and a warp's running sum of up to kWarpStage of them are
+    // 32-bit: the data graph's largest row bounds both, and caps the fan-out.
     const uint64_t row_max = std::max<uint64_t>(g.max_degree, 1);
     if (row_max * kWarpStage > 0xffffffffull) {
         err = "a data row of " + std::to_string(g.max_degree) + " entries exceeds the level step's 32-bit slice sums";
         return GFSM_ERR_TOO_LARGE;
     }
-    const uint64_t class_cap = 0xffffffffull / (row_max * kWarpStage);
+    const uint64_t fan_cap = 0xffffffffull / (row_max * kWarpStage);
+    std::vector<uint32_t> root_rep, fan_list, final_rep(na);
+    for (uint32_t i = 0; i < na; ++i) final_rep[i] = i;
     if (share) {
-        std::map<std::string, uint32_t> cls;  // prefix -> its class that still has room
-        for (uint32_t i = 0; i < na; ++i) {
-            const std::string key(reinterpret_cast<const char *>(&dq[i].lv[0]), 2 * sizeof(DLevel));
-            auto it = cls.find(key);
-            if (it == cls.end() || cls_members[it->second].size() >= class_cap) {
-                cls[key] = (uint32_t)cls_members.size();
-                cls_members.emplace_back();
-                it = cls.find(key);
+        // members of a node grouped by their plan at depth d, each group's
+        // members ascending, groups ordered by representative
+        auto split = [&](const std::vector<uint32_t> &mem, uint32_t d) {
+            std::map<std::string, std::vector<uint32_t>> by;
+            for (uint32_t i : mem) by[std::string(reinterpret_cast<const char *>(&dq[i].lv[d]), sizeof(DLevel))].push_back(i);
+            std::vector<std::vector<uint32_t>> out;
+            out.reserve(by.size());
+            for (auto &kv : by) out.push_back(std::move(kv.second));
+            std::sort(out.begin(), out.end(), [](const std::vector<uint32_t> &x, const std::vector<uint32_t> &y) {
+                return x[0] < y[0];
+            });
+            return out;
+        };
+        std::vector<uint32_t> all(na);
+        for (uint32_t i = 0; i < na; ++i) all[i] = i;
+        std::vector<std::vector<uint32_t>> level = split(all, 0);
+        for (const auto &n : level) root_rep.push_back(n[0]);
+        for (uint32_t d = 0; !level.empty() && share; ++d) {
+            std::vector<std::vector<uint32_t>> next;
+            for (auto &n : level) {
+                const uint32_t r = n[0];
+                if (dq[r].lv[d].final_) {
+                    for (uint32_t m : n) final_rep[m] = r;
+                    continue;
+                }
+                auto kids = split(n, d + 1);
+                if (kids.size() > fan_cap || kids.size() > 0xffffu) {  // too wide for the 32-bit slice sums
+                    share = false;
+                    break;
+                }
+                if (kids.size() > 1) {
+                    dq[r].lv[d].fan_count = (uint16_t)kids.size();
+                    dq[r].lv[d].fan_start = (uint32_t)fan_list.size();
+                    for (const auto &k : kids) fan_list.push_back(k[0]);
+                }
+                for (auto &k : kids) next.push_back(std::move(k));
             }
-            cls_members[it->second].push_back(i);
+            level.swap(next);
         }
-        root_base = na;
-        for (const auto &mem : cls_members) {
-            DQuery cq = dq[mem[0]];
-            if (cq.k > 2) cq.lv[1].fanout_next = 1;
-            ent.push_back(cq);
-            csize.push_back((uint32_t)mem.size());
-            mstart.push_back((uint32_t)members.size());
-            members.insert(members.end(), mem.begin(), mem.end());
-            root_lo.push_back(rlo[mem[0]]);
-            root_hi.push_back(rhi[mem[0]]);
+        if (!share) {
+            for (DQuery &q : dq)
+                for (DLevel &l : q.lv) l.fan_count = 0, l.fan_start = 0;
+            fan_list.clear();
+            root_rep.clear();
+            for (uint32_t i = 0; i < na; ++i) final_rep[i] = i;
         }
-    } else {
-        root_lo = rlo;
-        root_hi = rhi;
     }
-    const uint32_t ne = (uint32_t)ent.size();       // entities
-    const uint32_t nr = (uint32_t)root_lo.size();   // root-level parents
-    if (members.empty()) members.push_back(0);
+    if (!share)
+        for (uint32_t i = 0; i < na; ++i) root_rep.push_back(i);
+    const uint32_t ne = na;                        // count slots: one per query (representatives)
+    const uint32_t nr = (uint32_t)root_rep.size();  // root-level parents
+    if (fan_list.empty()) fan_list.push_back(0);
 
     // arena layout: plans | counts | step counts | root coff | root cstart |
-    //               class sizes | member starts | members | mapping rows | depth buffers
+    //               root representatives | fan list | mapping rows | depth buffers
     auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
     const uint64_t plans_bytes = (uint64_t)ne * sizeof(DQuery);
     const uint64_t head = al(plans_bytes) + 2 * al((uint64_t)ne * 8) + al(((uint64_t)nr + 1) * 8) +
-                          al((uint64_t)nr * 4) + 2 * al((uint64_t)ne * 4) + al((uint64_t)members.size() * 4) +
-                          al(rows_bytes);
+                          2 * al((uint64_t)nr * 4) + al((uint64_t)fan_list.size() * 4) + al(rows_bytes);
     uint64_t budget = arena_cap;
     if (budget <= head + (1ull << 20) * dmax) return GFSM_ERR_NOMEM;
     gfsm_status rc = ensure_arena(budget, err);
@@ -1223,34 +1248,32 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     p += al(((uint64_t)nr + 1) * 8);
     uint32_t *d_rcstart = reinterpret_cast<uint32_t *>(p);
     p += al((uint64_t)nr * 4);
-    uint32_t *d_csize = reinterpret_cast<uint32_t *>(p);
-    p += al((uint64_t)ne * 4);
-    uint32_t *d_mstart = reinterpret_cast<uint32_t *>(p);
-    p += al((uint64_t)ne * 4);
-    uint32_t *d_members = reinterpret_cast<uint32_t *>(p);
-    p += al((uint64_t)members.size() * 4);
+    uint32_t *d_root_rep = reinterpret_cast<uint32_t *>(p);
+    p += al((uint64_t)nr * 4);
+    uint32_t *d_fan_list = reinterpret_cast<uint32_t *>(p);
+    p += al((uint64_t)fan_list.size() * 4);
     uint32_t *d_rows = rows_out ? reinterpret_cast<uint32_t *>(p) : nullptr;
     p += al(rows_bytes);
 
     std::vector<unsigned long long> rcoff(nr + 1, 0);
-    for (uint32_t i = 0; i < nr; ++i) rcoff[i + 1] = rcoff[i] + (root_hi[i] - root_lo[i]);
-    ECHECK(cudaMemcpyAsync(d_plans, ent.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
+    std::vector<uint32_t> rcstart(nr);
+    for (uint32_t i = 0; i < nr; ++i) {
+        rcstart[i] = rlo[root_rep[i]];
+        rcoff[i + 1] = rcoff[i] + (rhi[root_rep[i]] - rlo[root_rep[i]]);
+    }
+    ECHECK(cudaMemcpyAsync(d_plans, dq.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
     ECHECK(cudaMemsetAsync(d_counts, 0, (uint64_t)ne * 8, stream));
     ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)nr + 1) * 8, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_rcstart, root_lo.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_csize, csize.data(), (uint64_t)ne * 4, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_mstart, mstart.data(), (uint64_t)ne * 4, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_members, members.data(), (uint64_t)members.size() * 4, cudaMemcpyHostToDevice,
+    ECHECK(cudaMemcpyAsync(d_rcstart, rcstart.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_root_rep, root_rep.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
+    ECHECK(cudaMemcpyAsync(d_fan_list, fan_list.data(), (uint64_t)fan_list.size() * 4, cudaMemcpyHostToDevice,
                            stream));
     ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
-    st.h2d_bytes += plans_bytes + ((uint64_t)nr + 1) * 8 + (uint64_t)nr * 4 + (uint64_t)ne * 8 +
-                    (uint64_t)members.size() * 4;
-    // per-query totals from the per-entity counts: a class that ends at a
-    // shared depth counted once for all of its members
+    st.h2d_bytes += plans_bytes + ((uint64_t)nr + 1) * 8 + 2 * (uint64_t)nr * 4 + (uint64_t)fan_list.size() * 4;
+    // per-query totals: every member of a final node gets its representative's count
     auto gather_counts = [&](const std::vector<unsigned long long> &cnt) {
-        std::vector<unsigned long long> out(cnt.begin(), cnt.begin() + na);
-        for (size_t c = 0; c < cls_members.size(); ++c)
-            for (uint32_t m : cls_members[c]) out[m] += cnt[na + c];
+        std::vector<unsigned long long> out(na);
+        for (uint32_t i = 0; i < na; ++i) out[i] = cnt[final_rep[i]];
         return out;
     };
     ECHECK(cudaEventRecord(ev_begin, stream));
@@ -1318,7 +1341,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         c.root_cstart = d_rcstart;
         c.counts = d_counts;
         c.nq = ne;
-        c.share_depth = share ? 2 : 0;
         c.max_scan = max_scan;
         c.max_candidates = lim.max_candidates;
         c.dmax = dmax;
@@ -1332,10 +1354,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_out = d_rows;
         a.max_rows = max_rows;
         a.rows_ctr = rows_ctr;
-        a.root_base = root_base;
-        a.csize = d_csize;
-        a.mstart = d_mstart;
-        a.members = d_members;
+        a.root_rep = d_root_rep;
+        a.fan_list = d_fan_list;
         Ctl *d_ctl = static_cast<Ctl *>(ctl);
         ECHECK(cudaMemcpyAsync(d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         st.h2d_bytes += sizeof(Ctl);
@@ -1434,11 +1454,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_out = d_rows;
         a.max_rows = max_rows;
         a.rows_ctr = rows_ctr;
-        a.root_base = root_base;
-        a.fanout = share && d == 2;
-        a.csize = d_csize;
-        a.mstart = d_mstart;
-        a.members = d_members;
+        a.root_rep = d_root_rep;
+        a.fan_list = d_fan_list;
         k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, ne), 256), 256, 0, stream>>>(
             a.pcoff, a.np, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts, ne);
         ECHECK(cudaEventRecord(ev0, stream));
@@ -1606,6 +1623,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     unsigned long long *d_count = reinterpret_cast<unsigned long long *>(p);
     unsigned long long *d_rcoff = d_count + 4;
     uint32_t *d_rcstart = reinterpret_cast<uint32_t *>(d_count + 8);
+    uint32_t *d_root_rep = d_rcstart + 4;  // the single root parent is query 0 of the plan array
     p += 256;
     const uint64_t used = (uint64_t)(p - scratch);
     const uint64_t share = dmax ? ((kNoAllocScratchBytes - used) / dmax) & ~255ull : 0;
@@ -1634,7 +1652,8 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     if (cudaMemcpyAsync(d_plan, &dq, sizeof(DQuery), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_rcoff, rc2, sizeof(rc2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_rcstart, &rlo, 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemsetAsync(d_count, 0, 8, st) != cudaSuccess || cudaMemsetAsync(rows_ctr, 0, 4, st) != cudaSuccess)
+        cudaMemsetAsync(d_count, 0, 8, st) != cudaSuccess || cudaMemsetAsync(d_root_rep, 0, 4, st) != cudaSuccess ||
+        cudaMemsetAsync(rows_ctr, 0, 4, st) != cudaSuccess)
         return GFSM_ERR_CUDA;
 
     const uint64_t max_scan = std::min<uint64_t>(lim.max_scan_size, (uint64_t)kNoAllocTiles * TILE);
@@ -1688,6 +1707,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         a.counts = d_count;
         a.result = d_result;
         a.rows_ctr = rows_ctr;
+        a.root_rep = d_root_rep;
         // one query: a step either counts (last level) or emits, so a re-run
         // step never counts twice and the count goes straight to the total
         k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(

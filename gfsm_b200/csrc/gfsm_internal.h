@@ -82,10 +82,15 @@ struct alignas(16) DLevel {
     uint8_t anchor_lab;        // label of the anchor requirement
     uint8_t final_;            // depth == k-1
     uint8_t anchor_check;      // anchor requirement needs a row search (multi-edge data)
-    uint8_t fanout_next;       // depth+1 fans a shared class out to its member queries
-    uint8_t pad1;
+    uint8_t pad0, pad1;
     uint8_t req_pos[MAXQ];     // tuple position, or REQ_SELF
     uint8_t req_lab[MAXQ];
+    // shared-prefix trie (set on a node's representative): the node's child
+    // nodes at depth+1 are fan_list[fan_start, fan_start + fan_count) when it
+    // has more than one
+    uint16_t fan_count;
+    uint16_t pad2;
+    uint32_t fan_start;
 };
 static_assert(sizeof(DLevel) == 64, "DLevel layout");
 
