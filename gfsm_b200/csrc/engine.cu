@@ -245,7 +245,7 @@ using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
 using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
 using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
 // Survivors one warp stages per tile, at most; their slice counts are
-// summed in 32 bits (see the class-size cap in Engine::run).
+// summed in 32 bits (see the trie fan-out cap in Engine::run).
 constexpr uint64_t kWarpStage = 128;
 static_assert(Geo0::WC <= kWarpStage && Geo1::WC <= kWarpStage && Geo2::WC <= kWarpStage && Geo3::WC <= kWarpStage,
               "a warp stages at most kWarpStage survivors");
