@@ -22,6 +22,7 @@ With N > 1 every rank runs its own batch (weak scaling, no collective on the
 data path); value = all ranks' queries / max-over-ranks time.
 """
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -349,6 +350,8 @@ def run_ours(args, rank, world, local, pg):
     plain = None
     if not args.no_plain:
         lat = []
+        gc.collect()
+        gc.disable()  # no collector pauses inside the latency samples
         t0 = time.perf_counter()
         plain_counts = []
         for p in plans:
@@ -357,6 +360,7 @@ def run_ours(args, rank, world, local, pg):
             lat.append((time.perf_counter() - a) * 1000.0)
             plain_counts.append(c)
         t_plain = time.perf_counter() - t0
+        gc.enable()
         exact = plain_counts == ref_counts.tolist()
         lat.sort()
         plain = {"queries_per_s": len(plans) / t_plain, "p50_ms": lat[len(lat) // 2],
@@ -370,6 +374,8 @@ def run_ours(args, rank, world, local, pg):
             n = min(len(plans), max(200, int(rate * 2.0)))
             srv = ctx.serve(data, slots=2, max_batch=256)
             gaps = rng.exponential(1.0 / rate, n)
+            gc.collect()
+            gc.disable()
             t0 = time.perf_counter()
             nxt = t0
             for i in range(n):
@@ -382,6 +388,7 @@ def run_ours(args, rank, world, local, pg):
                 srv.submit(plans[i], i)
             srv.drain(120000)
             wall = time.perf_counter() - t0
+            gc.enable()
             res = srv.poll(n + 10)
             srv.stop()
             ls = sorted(r["done_ms"] - r["submit_ms"] for r in res)

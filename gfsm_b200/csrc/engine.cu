@@ -1092,7 +1092,8 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
     std::vector<uint64_t> cnt(ns);
     // Samples under 2 ms of device time are launch-bound and their timings
     // mostly noise: keep the default there.  Elsewhere another geometry must
-    // beat the default by 3% to be chosen.
+    // beat the default by 2% to be chosen (repeat timings of a sample agree
+    // within ~0.5%).
     int best = 0;
     double base_ms = 0.0, best_ms = 1e300;
     for (int v = 0; v < kVariants; ++v) {
@@ -1102,7 +1103,7 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
             base_ms = s.device_ms;
             if (base_ms < 2.0) break;
         }
-        if (s.device_ms < best_ms && (v == 0 || s.device_ms < 0.97 * base_ms)) {
+        if (s.device_ms < best_ms && (v == 0 || s.device_ms < 0.98 * base_ms)) {
             best_ms = s.device_ms;
             best = v;
         }
