@@ -336,7 +336,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
         q &= ~kBranch;
         const DLevel *P = &a.plans[q].lv[d - 1];
         const unsigned long long pn = t.win ? t.win[lo + 1] : __ldg(a.pcoff + p + 1);
-        const uint32_t slen = (uint32_t)((pn - pc) / P->fan_count);
+        const uint32_t slen = (uint32_t)(pn - pc) / P->fan_count;  // the fan-out cap keeps pn - pc < 2^32
         const uint32_t j = local / slen;
         local -= j * slen;
         q = __ldg(a.fan_list + P->fan_start + j);
