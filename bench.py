@@ -253,11 +253,19 @@ def run_ours(args, rank, world, local, pg):
     g, qs = make_workload(rank, args.queries)
     s, d = g.directed()
     data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel).to_device()
+    # the batch's host input: every query's directed edge list and vertex
+    # labels, in flat arrays (query i: edges eoff[i]:eoff[i+1], nv[i] labels)
     qdir = [(q.n,) + tuple(q.directed()) + (q.vlabel,) for q in qs]
+    q_nv = np.array([n for n, _, _, _ in qdir], np.uint32)
+    q_eoff = np.zeros(len(qdir) + 1, np.uint64)
+    np.cumsum([len(a) for _, a, _, _ in qdir], out=q_eoff[1:])
+    q_src = np.concatenate([a for _, a, _, _ in qdir]).astype(np.uint32)
+    q_dst = np.concatenate([b for _, _, b, _ in qdir]).astype(np.uint32)
+    q_vl = np.concatenate([vl for _, _, _, vl in qdir]).astype(np.uint32)
 
-    def plans_from_host():
+    def plans_from_host(for_data=None):
         # every query's edge list -> plan, in one C call
-        return ctx.prepare_queries((n, a, b, None, vl) for n, a, b, vl in qdir)
+        return ctx.prepare_queries_flat(q_nv, q_eoff, q_src, q_dst, None, q_vl, for_data)
 
     plans = plans_from_host()
 
@@ -320,8 +328,7 @@ def run_ours(args, rank, world, local, pg):
         counts2, st2 = ctx.batch_count(p2, data)
         h2d += st2["h2d_bytes"]
         d2h += st2["d2h_bytes"]
-        for p in p2:
-            p.close()
+        p2.close()
     t_e2e = max_over_ranks(pg, time.perf_counter() - t0, local)
     assert counts2.tolist() == ref_counts.tolist()
     e2e = total_queries / t_e2e
@@ -330,7 +337,7 @@ def run_ours(args, rank, world, local, pg):
     # the headline above keeps the reference's order
     planner = None
     if not args.no_planner:
-        p3 = ctx.prepare_queries(((n, a, b, None, vl) for n, a, b, vl in qdir), data)
+        p3 = plans_from_host(data)
         ms3 = []
         for i in range(args.warmup + args.steps):
             flush_l2()
@@ -342,8 +349,7 @@ def run_ours(args, rank, world, local, pg):
                    "reference_order_candidates": int(st["candidates"]),
                    "data_aware_candidates": int(st3["candidates"]),
                    "data_aware_plans": int(sum(p.info()["planner"] for p in p3)), "exact": True}
-        for p in p3:
-            p.close()
+        p3.close()
 
     # -- plain form: one query at a time
     exact = True

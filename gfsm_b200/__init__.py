@@ -98,6 +98,7 @@ class Plan:
     def __init__(self, ctx, handle):
         self._ctx = ctx
         self._h = C.c_void_p(handle)
+        self._owned = True  # False for a view into a PlanBatch (the batch destroys it)
 
     @property
     def handle(self):
@@ -128,9 +129,50 @@ class Plan:
         return cols
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             self._ctx._lib.gfsm_plan_destroy(self._h)
-            self._h = C.c_void_p(None)
+        self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PlanBatch:
+    """The plans of a batch as one object: the C handles in one array, passed
+    to gfsm_batch_count as they are.  Indexing gives Plan views (owned by the
+    batch); close() destroys every plan."""
+
+    def __init__(self, ctx, arr, n):
+        self._ctx = ctx
+        self._arr = arr
+        self._n = n
+
+    def __len__(self):
+        return self._n
+
+    def __getitem__(self, i):
+        if not -self._n <= i < self._n:
+            raise IndexError(i)
+        p = Plan.__new__(Plan)
+        p._ctx = self._ctx
+        p._h = C.c_void_p(self._arr[i % self._n])
+        p._owned = False
+        return p
+
+    def __iter__(self):
+        return (self[i] for i in range(self._n))
+
+    def close(self):
+        if self._arr is not None:
+            destroy = self._ctx._lib.gfsm_plan_destroy
+            for h in self._arr:
+                if h:
+                    destroy(C.c_void_p(h))
+            self._arr = None
+            self._n = 0
 
     def __del__(self):
         try:
@@ -231,27 +273,35 @@ class GFSM:
         queries: iterable of (n, src, dst, elabel or None, vlabel or None),
         directed edge lists with ids local to each query.  The labels must be
         given for all queries or for none.  With `data`, each plan is
-        gfsm_query_prepare_for's (data-aware order where it is allowed)."""
+        gfsm_query_prepare_for's (data-aware order where it is allowed).
+        Returns a PlanBatch."""
         queries = list(queries)
         nq = len(queries)
-        if nq == 0:
-            return []
         nv = np.fromiter((int(q[0]) for q in queries), np.uint32, nq)
         ne = np.fromiter((len(q[1]) for q in queries), np.uint64, nq)
         eoff = np.zeros(nq + 1, np.uint64)
         np.cumsum(ne, out=eoff[1:])
-        cat = lambda i: np.ascontiguousarray(np.concatenate([np.asarray(q[i], np.uint32) for q in queries]),
-                                             np.uint32) if queries[0][i] is not None else None
-        src, dst, el, vl = cat(1), cat(2), cat(3), cat(4)
+        cat = lambda i: np.concatenate([np.asarray(q[i], np.uint32) for q in queries]) \
+            if nq and queries[0][i] is not None else None
+        return self.prepare_queries_flat(nv, eoff, cat(1), cat(2), cat(3), cat(4), data)
+
+    def prepare_queries_flat(self, nv, eoff, src, dst, elabel=None, vlabel=None, data=None):
+        """prepare_queries over a batch already in flat arrays: query i has
+        nv[i] vertices and the edges eoff[i]:eoff[i+1] of src/dst/elabel; its
+        vertex labels are the next nv[i] entries of vlabel."""
+        nq = len(nv)
+        out = (C.c_void_p * max(nq, 1))()
+        if nq == 0:
+            return PlanBatch(self, out, 0)
+        u32 = lambda a: None if a is None else np.ascontiguousarray(a, np.uint32)
+        nv, src, dst, elabel, vlabel = u32(nv), u32(src), u32(dst), u32(elabel), u32(vlabel)
+        eoff = np.ascontiguousarray(eoff, np.uint64)
         ptr = lambda a: a.ctypes.data_as(_lib.u32p) if a is not None and len(a) else None
-        if src is not None and len(src) == 0:
-            src = dst = None
-        out = (C.c_void_p * nq)()
         failed = C.c_int(-1)
         self._check(self._lib.gfsm_query_prepare_batch(
             self._h, nq, nv.ctypes.data_as(_lib.u32p), eoff.ctypes.data_as(_lib.u64p), ptr(src), ptr(dst),
-            ptr(el), ptr(vl), data.handle if data is not None else None, out, C.byref(failed)))
-        return [Plan(self, out[i]) for i in range(nq)]
+            ptr(elabel), ptr(vlabel), data.handle if data is not None else None, out, C.byref(failed)))
+        return PlanBatch(self, out, nq)
 
     # -- matching -------------------------------------------------------------
     def match_count(self, plan, data):
@@ -280,7 +330,10 @@ class GFSM:
         return rows[: nr.value], cnt.value
 
     def batch_count(self, plans, data):
-        arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
+        if isinstance(plans, PlanBatch):
+            arr = plans._arr
+        else:
+            arr = (C.c_void_p * max(len(plans), 1))(*[p.handle.value for p in plans])
         counts = np.zeros(max(len(plans), 1), np.uint64)
         st = Stats()
         self._check(self._lib.gfsm_batch_count(self._h, arr, len(plans), data.handle,

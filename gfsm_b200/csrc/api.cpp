@@ -43,13 +43,18 @@ Engine *ctx_engine(gfsm_ctx *ctx, const DeviceGraph &g, gfsm_status &rc, std::st
     }
     // MEMLIMIT covers the data graph, the engine's fixed buffers and the arena.
     const uint64_t used = g.bytes + e->small_bytes;
-    uint64_t cap = ctx->lim.mem_limit > used ? ctx->lim.mem_limit - used : 0;
+    const uint64_t lim_cap = ctx->lim.mem_limit > used ? ctx->lim.mem_limit - used : 0;
+    uint64_t cap = lim_cap;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         uint64_t avail = (uint64_t)free_b + e->arena_bytes;
         avail = avail > (1ull << 30) ? avail - (1ull << 30) : avail / 2;
         cap = std::min(cap, avail);
     }
+    // Keep an arena that MEMLIMIT still allows: free-memory readings move a
+    // little between calls, and re-allocating a multi-GB arena for that costs
+    // tens of milliseconds.  Grow it only for 25% more room.
+    if (e->arena && e->arena_bytes <= lim_cap && cap < e->arena_bytes + e->arena_bytes / 4) cap = e->arena_bytes;
     if (e->arena && e->arena_bytes > cap) {
         cudaFree(e->arena);
         e->arena = nullptr;

@@ -35,6 +35,8 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
+#include <unordered_map>
 
 #include "engine.h"
 
@@ -1127,20 +1129,35 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<DQuery> dq;
     std::vector<int> active;
     std::vector<uint32_t> rlo, rhi;
-    dq.reserve(nq);
     uint32_t dmax = 0;
-    for (int i = 0; i < nq; ++i) {
-        DQuery q;
-        uint32_t lo = 0, hi = 0;
-        bool never = false;
-        gfsm_status rc = build_dquery(*plans[i], g, lim, q, lo, hi, never);
-        if (rc != GFSM_OK) return rc;
-        if (never) continue;
-        dq.push_back(q);
-        active.push_back(i);
-        rlo.push_back(lo);
-        rhi.push_back(hi);
-        dmax = std::max(dmax, q.k - 1);
+    {
+        // independent per query: large batches use a few host threads
+        std::vector<DQuery> all(nq);
+        std::vector<uint32_t> lo(nq), hi(nq);
+        std::vector<char> never(nq, 0);
+        std::vector<gfsm_status> qrc(nq, GFSM_OK);
+        const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), nq / 512));
+        auto work = [&](int t) {
+            for (int i = t; i < nq; i += nt) {
+                bool nv = false;
+                qrc[i] = build_dquery(*plans[i], g, lim, all[i], lo[i], hi[i], nv);
+                never[i] = nv;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto &th : pool) th.join();
+        dq.reserve(nq);
+        for (int i = 0; i < nq; ++i) {
+            if (qrc[i] != GFSM_OK) return qrc[i];
+            if (never[i]) continue;
+            dq.push_back(all[i]);
+            active.push_back(i);
+            rlo.push_back(lo[i]);
+            rhi.push_back(hi[i]);
+            dmax = std::max(dmax, all[i].k - 1);
+        }
     }
     const uint32_t na = (uint32_t)active.size();
     if (na == 0) {
@@ -1175,17 +1192,37 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<uint32_t> root_rep, fan_list, final_rep(na);
     for (uint32_t i = 0; i < na; ++i) final_rep[i] = i;
     if (share) {
-        // members of a node grouped by their plan at depth d, each group's
-        // members ascending, groups ordered by representative
+        // members of a node grouped by their plan at depth d (hash of the
+        // 64 plan bytes, equality checked bytewise), each group's members
+        // ascending, groups ordered by representative -- the first member
+        // seen, as members arrive ascending
+        auto lv_hash = [&](uint32_t i, uint32_t d) {
+            uint64_t w[sizeof(DLevel) / 8];
+            std::memcpy(w, &dq[i].lv[d], sizeof(DLevel));
+            uint64_t h = 0x9e3779b97f4a7c15ull;
+            for (uint64_t x : w) h = (h ^ x) * 0xff51afd7ed558ccdull, h ^= h >> 32;
+            return h;
+        };
         auto split = [&](const std::vector<uint32_t> &mem, uint32_t d) {
-            std::map<std::string, std::vector<uint32_t>> by;
-            for (uint32_t i : mem) by[std::string(reinterpret_cast<const char *>(&dq[i].lv[d]), sizeof(DLevel))].push_back(i);
             std::vector<std::vector<uint32_t>> out;
-            out.reserve(by.size());
-            for (auto &kv : by) out.push_back(std::move(kv.second));
-            std::sort(out.begin(), out.end(), [](const std::vector<uint32_t> &x, const std::vector<uint32_t> &y) {
-                return x[0] < y[0];
-            });
+            std::unordered_multimap<uint64_t, uint32_t> by;  // hash -> group
+            by.reserve(mem.size() * 2);
+            for (uint32_t i : mem) {
+                const uint64_t h = lv_hash(i, d);
+                uint32_t gi = ~0u;
+                auto rg = by.equal_range(h);
+                for (auto it = rg.first; it != rg.second; ++it)
+                    if (!std::memcmp(&dq[out[it->second][0]].lv[d], &dq[i].lv[d], sizeof(DLevel))) {
+                        gi = it->second;
+                        break;
+                    }
+                if (gi == ~0u) {
+                    gi = (uint32_t)out.size();
+                    out.emplace_back();
+                    by.emplace(h, gi);
+                }
+                out[gi].push_back(i);
+            }
             return out;
         };
         std::vector<uint32_t> all(na);

@@ -169,4 +169,30 @@ def test_batch_planning_reports_the_failing_query(host_ctx):
     with pytest.raises(gfsm_b200.GFSMError) as ei:
         host_ctx.prepare_queries([tri, bad])
     assert ei.value.status == 233  # GFSM_ERR_INVALID_DATA
-    assert host_ctx.prepare_queries([]) == []
+    assert len(host_ctx.prepare_queries([])) == 0
+
+
+def test_flat_batch_planning_and_plan_batch(host_ctx):
+    """prepare_queries_flat over flat arrays gives the per-query plans; a
+    PlanBatch indexes as Plan views and closes every plan once."""
+    from gfsm_b200 import synth
+    g = synth.grid(30, 0.05, 0.02, seed=2)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=4)
+    qs = [synth.rw_query(g, 3 + i % 6, seed=300 + i)[0] for i in range(50)]
+    dirs = [q.directed() for q in qs]
+    nv = np.array([q.n for q in qs], np.uint32)
+    eoff = np.zeros(len(qs) + 1, np.uint64)
+    np.cumsum([len(a) for a, _ in dirs], out=eoff[1:])
+    src = np.concatenate([a for a, _ in dirs])
+    dst = np.concatenate([b for _, b in dirs])
+    vl = np.concatenate([q.vlabel for q in qs])
+    batch = host_ctx.prepare_queries_flat(nv, eoff, src, dst, None, vl)
+    assert len(batch) == len(qs)
+    for q, (a, b), p in zip(qs, dirs, batch):
+        one = host_ctx.pre_process_query(host_ctx.graph_from_edges(q.n, a, b, None, q.vlabel))
+        assert p.tables()["order"].tolist() == one.tables()["order"].tolist()
+        assert p.tables()["reqs"].tolist() == one.tables()["reqs"].tolist()
+        p.close()  # a view: does not destroy the batch's plan
+    assert batch[-1].tables()["k"] == qs[-1].n
+    batch.close()
+    assert len(batch) == 0
