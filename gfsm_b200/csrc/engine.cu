@@ -941,6 +941,9 @@ void Engine::release() {
     if (arena) cudaFree(arena);
     if (small) cudaFree(small);
     if (h_result) cudaFreeHost(h_result);
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
+    h_stage_bytes = 0;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (ev_begin) cudaEventDestroy(ev_begin);
@@ -1291,23 +1294,43 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     uint32_t *d_fan_list = reinterpret_cast<uint32_t *>(p);
     p += al((uint64_t)fan_list.size() * 4);
     uint32_t *d_rows = rows_out ? reinterpret_cast<uint32_t *>(p) : nullptr;
+    const uint64_t head_used = (uint64_t)(p - static_cast<char *>(arena));  // everything the call sends
     p += al(rows_bytes);
 
-    std::vector<unsigned long long> rcoff(nr + 1, 0);
-    std::vector<uint32_t> rcstart(nr);
-    for (uint32_t i = 0; i < nr; ++i) {
-        rcstart[i] = rlo[root_rep[i]];
-        rcoff[i + 1] = rcoff[i] + (rhi[root_rep[i]] - rlo[root_rep[i]]);
+    // The head (plans, zeroed counts, root tables, fan list) is laid out in a
+    // pinned staging buffer exactly as in the arena and sent with one copy.
+    // A copy of an earlier call (one that returned early) may still read it.
+    ECHECK(cudaStreamSynchronize(stream));
+    if (h_stage_bytes < head_used) {
+        // grown geometrically: freeing pinned memory synchronises the device,
+        // and served slots see batches of every size
+        const uint64_t want = std::max<uint64_t>({head_used, 2 * h_stage_bytes, 1ull << 20});
+        if (h_stage) cudaFreeHost(h_stage);
+        h_stage = nullptr;
+        h_stage_bytes = 0;
+        ECHECK(cudaMallocHost(&h_stage, want));
+        h_stage_bytes = want;
     }
-    ECHECK(cudaMemcpyAsync(d_plans, dq.data(), plans_bytes, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemsetAsync(d_counts, 0, (uint64_t)ne * 8, stream));
-    ECHECK(cudaMemcpyAsync(d_rcoff, rcoff.data(), ((uint64_t)nr + 1) * 8, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_rcstart, rcstart.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_root_rep, root_rep.data(), (uint64_t)nr * 4, cudaMemcpyHostToDevice, stream));
-    ECHECK(cudaMemcpyAsync(d_fan_list, fan_list.data(), (uint64_t)fan_list.size() * 4, cudaMemcpyHostToDevice,
-                           stream));
+    char *hs = static_cast<char *>(h_stage);
+    auto host_of = [&](const void *dev) { return hs + (static_cast<const char *>(dev) - static_cast<char *>(arena)); };
+    std::memcpy(host_of(d_plans), dq.data(), plans_bytes);
+    std::memset(host_of(d_counts), 0, 2 * al((uint64_t)ne * 8));  // counts and step counts
+    {
+        unsigned long long *rcoff = reinterpret_cast<unsigned long long *>(host_of(d_rcoff));
+        uint32_t *rcstart = reinterpret_cast<uint32_t *>(host_of(d_rcstart));
+        rcoff[0] = 0;
+        for (uint32_t i = 0; i < nr; ++i) {
+            rcstart[i] = rlo[root_rep[i]];
+            rcoff[i + 1] = rcoff[i] + (rhi[root_rep[i]] - rlo[root_rep[i]]);
+        }
+    }
+    std::memcpy(host_of(d_root_rep), root_rep.data(), (uint64_t)nr * 4);
+    std::memcpy(host_of(d_fan_list), fan_list.data(), (uint64_t)fan_list.size() * 4);
+    const unsigned long long root_total =
+        reinterpret_cast<const unsigned long long *>(host_of(d_rcoff))[nr];
+    ECHECK(cudaMemcpyAsync(arena, h_stage, head_used, cudaMemcpyHostToDevice, stream));
     ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
-    st.h2d_bytes += plans_bytes + ((uint64_t)nr + 1) * 8 + 2 * (uint64_t)nr * 4 + (uint64_t)fan_list.size() * 4;
+    st.h2d_bytes += head_used;
     // per-query totals: every member of a final node gets its representative's count
     auto gather_counts = [&](const std::vector<unsigned long long> &cnt) {
         std::vector<unsigned long long> out(na);
@@ -1366,7 +1389,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     if (graph_driver) {
         Ctl c;
         std::memset(&c, 0, sizeof(c));
-        c.total[0] = rcoff[nr];
+        c.total[0] = root_total;
         c.np[0] = nr;
         for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = 1.0f;
         for (uint32_t i = 0; i < dmax; ++i) {
@@ -1439,7 +1462,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<double> ratio(dmax + 1, 1.0);
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) has_final[q.k - 1] = 1;
-    total[0] = rcoff[nr];
+    total[0] = root_total;
     np[0] = nr;
     uint32_t d = 0;
     float kms = 0.f;

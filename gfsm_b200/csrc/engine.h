@@ -22,6 +22,8 @@ struct Engine {
     uint32_t dir_tiles = 0;        // tile directory capacity (tiles per step)
     StepResult *d_result = nullptr;
     StepResult *h_result = nullptr;  // pinned
+    void *h_stage = nullptr;         // pinned staging of a call's arena head (plans, root tables, ...)
+    uint64_t h_stage_bytes = 0;
     uint32_t *tile_ctr = nullptr;
     uint32_t *rows_ctr = nullptr;
     uint32_t *tile_parent = nullptr;
