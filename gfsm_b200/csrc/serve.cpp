@@ -150,6 +150,10 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         if (rc != GFSM_OK) return rc;
         e->arena_cap = per_slot > e->small_bytes ? per_slot - e->small_bytes : 0;
         e->autotune = false;  // a request never waits for tuning runs
+        // pinned staging for a full batch's plans, so no request allocates it
+        const uint64_t stage = std::max<uint64_t>(1ull << 20, (uint64_t)c.max_batch * sizeof(DQuery) * 2);
+        if (cudaMallocHost(&e->h_stage, stage) != cudaSuccess) return GFSM_ERR_NOMEM;
+        e->h_stage_bytes = stage;
         s->engines.push_back(std::move(e));
     }
     s->slot_budget = c.frontier_bytes ? c.frontier_bytes : per_slot;
