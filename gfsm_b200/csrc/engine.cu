@@ -12,15 +12,19 @@
 //     vertex (rows are sorted by a degree-descending, label-grouped id, so
 //     the window is one contiguous slice found by two binary searches when
 //     the parent was produced);
-//   * tiles of 1024 candidates (256 threads x 4), so hub rows are split across
-//     tiles and every thread does the same amount of row work -- the load
-//     balance the reference's thread-per-parent hnGen lacks;
+//   * tiles of 512-1024 candidates (autotuned geometry), so hub rows are
+//     split across tiles and every thread does the same amount of row work --
+//     the load balance the reference's thread-per-parent hnGen lacks;
 //   * per candidate: injectivity against the parent tuple, the anchor's edge
-//     label, and a binary search in each other backward neighbour's row for
-//     the remaining requirements;
-//   * survivors are ranked with __ballot_sync/__popc, the tile's output
-//     offset (child count and next-level candidate count) comes from a
-//     decoupled look-back over tiles taken in launch order (bounded waits);
+//     label, and a search in each other backward neighbour's row for the
+//     remaining requirements;
+//   * survivors are ranked with __ballot_sync/__popc into shared memory, and
+//     the tile's output offset (child count and next-level candidate count)
+//     comes from one 64-bit atomic on the step's allocator word -- no tile
+//     waits for another;
+//   * a batch shares query prefixes through a trie of its plans: a tuple
+//     stands for every query of its trie node, and a branching node's
+//     candidates run over (child node, row offset);
 //   * children are written as full tuples (SoA columns) together with their
 //     own next-level candidate slice, so the next step needs no scan, no
 //     pointer chasing up a forest, and no separate compaction;
