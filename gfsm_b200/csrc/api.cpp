@@ -45,8 +45,13 @@ Engine *ctx_engine(gfsm_ctx *ctx, const DeviceGraph &g, gfsm_status &rc, std::st
     const uint64_t used = g.bytes + e->small_bytes;
     const uint64_t lim_cap = ctx->lim.mem_limit > used ? ctx->lim.mem_limit - used : 0;
     uint64_t cap = lim_cap;
+    // Free device memory is read when the arena is first sized and then every
+    // 1024th call (a chance to grow): the query goes through the driver,
+    // which other processes on the machine share, and it sometimes stalls
+    // for milliseconds -- too long for every call of a sub-millisecond query.
+    const bool probe = !e->arena || e->arena_bytes > lim_cap || (ctx->calls++ & 1023u) == 0;
     size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    if (probe && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         uint64_t avail = (uint64_t)free_b + e->arena_bytes;
         avail = avail > (1ull << 30) ? avail - (1ull << 30) : avail / 2;
         cap = std::min(cap, avail);
@@ -54,7 +59,8 @@ Engine *ctx_engine(gfsm_ctx *ctx, const DeviceGraph &g, gfsm_status &rc, std::st
     // Keep an arena that MEMLIMIT still allows: free-memory readings move a
     // little between calls, and re-allocating a multi-GB arena for that costs
     // tens of milliseconds.  Grow it only for 25% more room.
-    if (e->arena && e->arena_bytes <= lim_cap && cap < e->arena_bytes + e->arena_bytes / 4) cap = e->arena_bytes;
+    if (e->arena && e->arena_bytes <= lim_cap && (!probe || cap < e->arena_bytes + e->arena_bytes / 4))
+        cap = e->arena_bytes;
     if (e->arena && e->arena_bytes > cap) {
         cudaFree(e->arena);
         e->arena = nullptr;

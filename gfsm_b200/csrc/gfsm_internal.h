@@ -138,6 +138,7 @@ struct gfsm_ctx {
     std::string last_error;
     std::mutex mu;
     void *engine = nullptr;   // default gfsm::Engine (stream + frontier arena)
+    uint64_t calls = 0;       // matching calls on the default engine
 };
 
 namespace gfsm {
