@@ -464,3 +464,42 @@ def test_shared_prefixes_identical_queries_on_a_hub():
     counts, st = ctx.batch_count([tri] * 900, data)
     assert counts.tolist() == [one] * 900
     ctx.close()
+
+
+def test_trie_too_wide_for_row_size_runs_unshared():
+    """With a 2^24-entry row (a star), a trie node may not branch at all
+    (its fan-out times the row must fit 32-bit slice sums with 128 per warp);
+    three queries with the same root level but different depth-1 plans (their
+    depth-2 windows differ) would make the root node branch, so the call runs
+    unshared, and the counts equal one-at-a-time matching and the oracle."""
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    m = 1 << 24
+    leaves = np.arange(1, m + 1, dtype=np.uint32)
+    hub = np.zeros(m, np.uint32)
+    # a labelled grid component (labels 1..3) beside the label-0 star
+    comp = synth.grid(20, 0.0, 0.05, seed=41)
+    off = m + 1
+    cs, cd = comp.directed()
+    src = np.concatenate([hub, leaves, cs.astype(np.uint32) + off])
+    dst = np.concatenate([leaves, hub, cd.astype(np.uint32) + off])
+    vl = np.concatenate([np.zeros(m + 1, np.uint32), 1 + synth.vlabels(comp.n, 3, 0.0, seed=42)])
+    data = ctx.graph_from_edges(m + 1 + comp.n, src, dst, None, vl)
+    # paths a-b-c, planned b, a, c: b labelled 1, a 2, and c 1, 2 or 3
+    qs = []
+    for l3 in (1, 2, 3):
+        qvl = np.array([2, 1, l3], np.uint32)
+        qs.append((3, np.array([0, 1, 1, 2], np.uint32), np.array([1, 0, 2, 1], np.uint32), None, qvl))
+    plans = [ctx.pre_process_query(ctx.graph_from_edges(*q)) for q in qs]
+    alone = [ctx.match_count(p, data) for p in plans]
+    single = [c for c, _ in alone]
+    batch, st = ctx.batch_count(plans, data)
+    assert batch.tolist() == single and sum(single) > 0
+    # unshared: the batch processes exactly the candidates of the three calls
+    # (shared, the common root level would run once)
+    assert st["candidates"] == sum(s["candidates"] for _, s in alone)
+    # the oracle on the component alone (the star has no labels 1-3)
+    ccs, ccd = comp.directed()
+    cvl = vl[off:]
+    for (n, a, b, _, qvl), c in zip(qs, single):
+        assert c == O.bt_count(n, a, b, None, qvl, comp.n, ccs, ccd, None, cvl, vlabel_mode=True)
+    ctx.close()
