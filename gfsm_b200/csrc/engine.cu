@@ -657,7 +657,6 @@ struct Ctl {
     uint32_t d, dmax, emits, done, err;
 };
 
-constexpr uint32_t KERR_CAP = 16u;      // max_candidates reached
 
 // Chooses the next step (the host loop's logic); sets done when none is left.
 __device__ void ctl_plan(Ctl &c) {

@@ -109,7 +109,7 @@ struct StepResult {
     unsigned long long total_next;
     unsigned long long alg_bytes;
     unsigned long long alloc;
-    unsigned int err;          // KERR_* bits
+    unsigned int err;          // error bits a kernel may raise (none does today; the host checks them)
     unsigned int rows;         // mapping rows claimed (mapping mode)
     unsigned int tiles_done;   // tiles that have allocated (the last one publishes the totals)
     unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
@@ -121,10 +121,10 @@ constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candida
 // so the count never wraps (every candidate yields at most one child).
 constexpr unsigned long long kMaxEmitChunk = (1ull << (64 - kAllocShift)) - 1024;
 
-// Error bits raised by kernels (read by the host after each step).
+// Error bits of a schedule (the graph-driven controller sets them; the
+// host-driven loop checks the same conditions on the host).
 enum : uint32_t {
-    KERR_WINDOW = 2u,          // parent window larger than expected
-    KERR_BOUNDS = 4u,          // a vertex id out of range
+    KERR_CAP = 16u,            // the candidate cap (max_candidates) was reached, or one tile overflowed
 };
 
 }  // namespace gfsm
