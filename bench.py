@@ -427,6 +427,11 @@ def run_ours(args, rank, world, local, pg):
         cpu = {"value": done / el, "unit": "queries/s", "cores": co.threads, "kind": "port",
                "sample": f"first {done} queries of the batch (~15 s of host CPU), oracle restatement of the "
                          f"reference FFS algorithm"}
+        # the same on one core (a scalar port), over a ~5 s sample
+        c1 = CpuOracle(g, threads=1)
+        d1, e1, c1counts = c1.run(qs, budget_s=5.0)
+        exact = exact and c1counts == ref_counts[:d1].tolist()
+        cpu["single_core"] = {"value": d1 / e1, "unit": "queries/s", "cores": 1, "queries": d1}
 
     if rank == 0:
         line = {
