@@ -783,8 +783,13 @@ __global__ void k_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int first) {
 }
 
 // Graph node: first parent of every tile of the step (strided fixed grid).
-__global__ void k_part_g(int slot, const Ctl *ctl) {
-    const StepArgs &a = c_args[slot];
+// The graph kernels are instantiated per argument slot, so the slot's
+// fields are compile-time constant-bank operands like kernel parameters (a
+// runtime slot index turns every field read into a load: the R-MAT triangle
+// ran 10% slower that way).
+template <int SLOT>
+__global__ void k_part_g(const Ctl *ctl) {
+    const StepArgs &a = c_args[SLOT];
     const unsigned long long ncand = a.cend - a.c0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ctl->nq; i += gridDim.x * blockDim.x)
         a.counts[i] = 0;
@@ -801,18 +806,31 @@ __global__ void k_part_g(int slot, const Ctl *ctl) {
 
 // Graph node: the level step on a fixed grid; every CTA takes tiles from the
 // step's tile queue.
-__global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g(int slot) {
+template <int SLOT>
+__global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g() {
     __shared__ StepSmem<Geo0> sm;
-    __shared__ uint32_t s_tile;
-    const StepArgs &a = c_args[slot];
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
-        __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= a.ntiles) break;
+    __shared__ uint32_t s_tile[2];
+    const StepArgs &a = c_args[SLOT];
+    // the next tile is fetched while this one runs (double-buffered: a slot
+    // is rewritten only after every thread has passed the barrier that
+    // follows its read)
+    if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.tile_ctr, 1u);
+    __syncthreads();
+    uint32_t tile = s_tile[0];
+    for (uint32_t it = 1; tile < a.ntiles; ++it) {
+        if (threadIdx.x == 0) s_tile[it & 1u] = atomicAdd(a.tile_ctr, 1u);
         if (a.depth == 0) step_tile<true, Geo0>(a, tile, sm);
         else step_tile<false, Geo0>(a, tile, sm);
+        __syncthreads();
+        tile = s_tile[it & 1u];
     }
+}
+
+template <int... S>
+const void *slot_kernel(int s, bool step) {
+    static const void *part[] = {(const void *)k_part_g<S>...};
+    static const void *stepk[] = {(const void *)k_step_g<S>...};
+    return step ? stepk[s] : part[s];
 }
 
 inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
@@ -989,7 +1007,7 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     {
         int sms = 0, per_sm = 0;
         ECHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_g, T, 0));
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_g<0>, T, 0));
         step_blocks = sms * std::max(per_sm, 1);
     }
     arg_slot = acquire_arg_slot();
@@ -1032,8 +1050,7 @@ gfsm_status Engine::build_graph(std::string &err) {
     int first = 1, next = 0, slot = arg_slot;
     void *a_first[] = {&cp, &h, &first};
     void *a_next[] = {&cp, &h, &next};
-    void *a_slot[] = {&slot};
-    void *a_part[] = {&slot, &cp};
+    void *a_part[] = {&cp};
     cudaKernelNodeParams kp{};
     kp.func = (void *)k_ctl;
     kp.gridDim = dim3(1);
@@ -1052,14 +1069,14 @@ gfsm_status Engine::build_graph(std::string &err) {
     if ((e = cudaGraphAddMemcpyNodeToSymbol(&b0, body, nullptr, 0, c_args, &cp->args, sizeof(StepArgs),
                                             (size_t)slot * sizeof(StepArgs), cudaMemcpyDeviceToDevice)) != cudaSuccess)
         return fail(e, "args copy node");
-    kp.func = (void *)k_part_g;
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, false));
     kp.gridDim = dim3((unsigned)step_blocks);
     kp.blockDim = dim3(256);
     kp.kernelParams = a_part;
     if ((e = cudaGraphAddKernelNode(&b1, body, &b0, 1, &kp)) != cudaSuccess) return fail(e, "partition node");
-    kp.func = (void *)k_step_g;
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, true));
     kp.blockDim = dim3(T);
-    kp.kernelParams = a_slot;
+    kp.kernelParams = nullptr;
     if ((e = cudaGraphAddKernelNode(&b2, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "step node");
     kp.func = (void *)k_ctl;
     kp.gridDim = dim3(1);
@@ -1391,6 +1408,15 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
 
     GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
+    // GFSM_SURVIVOR_GUESS: the survivor ratio assumed for a depth's first
+    // chunk (default 1: a first chunk never overflows).  A smaller guess takes
+    // larger first chunks -- fewer steps where survival is low, re-runs where
+    // it is not.  Later chunks follow the observed ratio either way.
+    const double ratio_init = [] {  // read per call: cheap, and tests change it
+        const char *v = getenv("GFSM_SURVIVOR_GUESS");
+        const double x = v && *v ? atof(v) : 1.0;
+        return x > 0.0 ? std::min(1.0, std::max(x, 1.0 / 8192.0)) : 1.0;
+    }();
     // the graph-driven schedule (falls back to the host loop if the graph
     // cannot be built, e.g. when every constant-memory argument slot is taken)
     const bool graph_driver = want_graph && build_graph(err) == GFSM_OK;
@@ -1399,7 +1425,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         std::memset(&c, 0, sizeof(c));
         c.total[0] = root_total;
         c.np[0] = nr;
-        for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = 1.0f;
+        for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = (float)ratio_init;
         for (uint32_t i = 0; i < dmax; ++i) {
             c.tup[i] = buf[i].tup;
             c.cap[i] = buf[i].cap;
@@ -1467,7 +1493,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         return GFSM_OK;
     }
     std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0);
-    std::vector<double> ratio(dmax + 1, 1.0);
+    std::vector<double> ratio(dmax + 1, ratio_init);
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) has_final[q.k - 1] = 1;
     total[0] = root_total;

@@ -333,17 +333,21 @@ def test_autotuner_choice_is_exact(monkeypatch):
 def test_mixed_batch_retries_count_once(monkeypatch):
     """A batch mixing query sizes under tight MEMLIMITs re-runs steps that
     overflow their level buffer; queries that end at such a step must still be
-    counted once (per-step count scratch, committed on acceptance).  A CTA-tile
-    geometry is pinned: its steps are large enough to overflow.  Unshared runs
-    (GFSM_SHARE=0) are the ones that overflow; shared runs must agree."""
+    counted once (per-step count scratch, committed on acceptance).  Children
+    are written in tile-completion order, so the chunking of later levels (and
+    whether a step overflows) varies from run to run; a survivor guess of 0.1%
+    makes every depth's first chunk far larger than its buffer, so steps do
+    overflow and are re-run.  Counts must equal the unconstrained run's,
+    shared and unshared."""
     monkeypatch.setenv("GFSM_TILE", "0")
+    monkeypatch.setenv("GFSM_SURVIVOR_GUESS", "0.001")
     g = synth.grid(200, 0.05, 0.05, seed=21)
     g.vlabel = synth.vlabels(g.n, 2, 0.0, seed=22)
     s, d = g.directed()
     results = []
     for share, mem in [(sh, m) for sh in ("0", "1") for m in (None, 24 << 20, 16 << 20, 12 << 20, 10 << 20)]:
         monkeypatch.setenv("GFSM_SHARE", share)
-        kw = {} if mem is None else dict(mem_limit=mem, max_scan_size=1 << 16)
+        kw = {} if mem is None else dict(mem_limit=mem, max_scan_size=1 << 20)
         ctx = gfsm_b200.GFSM(device=0, vertex_labels=1, **kw)
         data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
         plans = []
@@ -358,7 +362,7 @@ def test_mixed_batch_retries_count_once(monkeypatch):
     assert sum(ref) > 0
     for counts, retries, steps in results[1:]:
         assert counts == ref
-    assert max(r for _, r, _ in results[1:5]) > 0, [(r, st) for _, r, st in results]
+    assert min(r for _, r, _ in results[1:5]) > 0, [(r, st) for _, r, st in results]
 
 
 def test_shared_prefix_batches(monkeypatch):
