@@ -1087,6 +1087,7 @@ gfsm_status Engine::build_graph(std::string &err) {
         graph_exec = nullptr;
         return fail(e, "cudaGraphInstantiate");
     }
+    cudaGraphUpload(graph_exec, stream);  // its first launch does not pay the upload
     graph = g;
     return GFSM_OK;
 }

@@ -154,6 +154,14 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         const uint64_t stage = std::max<uint64_t>(1ull << 20, (uint64_t)c.max_batch * sizeof(DQuery) * 2);
         if (cudaMallocHost(&e->h_stage, stage) != cudaSuccess) return GFSM_ERR_NOMEM;
         e->h_stage_bytes = stage;
+        // the graph a single-query batch runs is built now, not on a request
+        // (if no argument slot is left, the slot runs the host-driven loop)
+        std::string gerr;
+        e->build_graph(gerr);
+        // and the slot's frontier arena: a first request must not pay a
+        // multi-GB cudaMalloc
+        rc = e->ensure_arena(e->arena_cap, err);
+        if (rc != GFSM_OK) return rc;
         s->engines.push_back(std::move(e));
     }
     s->slot_budget = c.frontier_bytes ? c.frontier_bytes : per_slot;
