@@ -299,7 +299,7 @@ def run_ours(args, rank, world, local, pg):
 
     # -- device-resident batched steps
     clocks = Clocks(local)
-    dev_ms, k_ms, alg, launches, cand = [], 0.0, 0, 0, 0
+    dev_ms, k_ms, alg, launches, step_launches, cand = [], 0.0, 0, 0, 0, 0
     barrier(pg)
     torch.cuda.synchronize(local)
     clocks.start()
@@ -310,7 +310,8 @@ def run_ours(args, rank, world, local, pg):
         dev_ms.append(st["device_ms"])
         k_ms += st["kernel_ms"]
         alg += st["alg_bytes"]
-        launches += 2 * st["steps"]
+        launches += st["launches"]          # every kernel of the call
+        step_launches += st["steps"]        # level-step kernels
         cand += st["candidates"]
     torch.cuda.synchronize(local)
     barrier(pg)
@@ -407,7 +408,7 @@ def run_ours(args, rank, world, local, pg):
     pk, pk_kind = peaks()
     achieved = alg / (k_ms / 1000.0) / 1e9 if k_ms else 0.0
     tr = traffic_record()
-    k_launches = launches // 2
+    k_launches = step_launches
     traffic = None
     if tr and k_launches:
         # measured DRAM bytes per candidate (small-case ncu capture) x candidates per launch

@@ -91,6 +91,7 @@ class Stats(C.Structure):
         ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64),
         ("tile_variant", C.c_int32),
+        ("launches", C.c_uint32),
     ]
 
     def as_dict(self):

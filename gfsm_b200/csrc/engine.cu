@@ -1467,6 +1467,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         st.steps = c.steps;
+        st.launches = (uint32_t)(1 + 3 * c.steps);  // first controller, then partition, step, controller per step
         st.retries = c.retries;
         st.candidates = c.candidates;
         st.expansions = c.expansions;
@@ -1557,6 +1558,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         ECHECK(cudaEventRecord(ev0, stream));
         launch_step(variant, d == 0, a, ntiles, stream);
         ECHECK(cudaGetLastError());
+        st.launches += 2;  // partition + level step
         ECHECK(cudaEventRecord(ev1, stream));
         ECHECK(cudaMemcpyAsync(h_result, d_result, sizeof(StepResult), cudaMemcpyDeviceToHost, stream));
         ECHECK(cudaStreamSynchronize(stream));
@@ -1584,8 +1586,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (trace)
             fprintf(stderr, "gfsm-step depth=%u cand=%llu children=%llu next=%llu tiles=%u ms=%.4f\n", d, chunk,
                     emits ? r.n_children : 0ull, emits ? r.total_next : 0ull, ntiles, ms);
-        if (has_final[d])
+        if (has_final[d]) {
             k_commit<<<(unsigned)div_up(ne, 256), 256, 0, stream>>>(d_counts, d_step_counts, ne);
+            st.launches += 1;
+        }
         st.candidates += chunk;
         st.expansions += r.n_children;
         if (lim.max_candidates && st.candidates > lim.max_candidates) {

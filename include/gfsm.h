@@ -87,6 +87,7 @@ typedef struct {
     uint64_t h2d_bytes;          /* host->device bytes copied by the call          */
     uint64_t d2h_bytes;          /* device->host bytes copied by the call          */
     int32_t  tile_variant;       /* tile geometry the autotuner chose (0..3)        */
+    uint32_t launches;           /* kernels the call launched (graph nodes included) */
 } gfsm_stats;
 
 typedef struct {
