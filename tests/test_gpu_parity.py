@@ -274,6 +274,10 @@ def test_device_and_host_drivers_agree(monkeypatch):
     assert dev_counts.tolist() == host_counts.tolist()
     for key in ("candidates", "expansions", "steps", "retries"):
         assert dev_st[key] == host_st[key], key
+    # kernels launched: partition + step per step (+ count commits) on the
+    # host loop; the graph's controller, partition, step and controller nodes
+    assert 2 * host_st["steps"] <= host_st["launches"] <= 3 * host_st["steps"]
+    assert dev_st["launches"] == 1 + 3 * dev_st["steps"]
     for (c1, s1), (c2, s2) in zip(host_single, dev_single):
         assert c1 == c2 and s1["candidates"] == s2["candidates"]
     assert host_st["steps"] > 20
