@@ -116,6 +116,16 @@ class Plan:
                                               header.ctypes.data_as(_lib.u32p), reqs.ctypes.data_as(_lib.u32p)))
         return {"k": k, "max_valency": mv, "order": order, "header": header, "reqs": reqs[: 2 * mv * k]}
 
+    def symmetry(self):
+        """(|Aut(Q)|, [(a, b), ...]): count embeddings with f(a) < f(b) for
+        every pair, times |Aut(Q)|, to get the full count."""
+        lib = self._ctx._lib
+        aut, n = C.c_uint64(), C.c_uint32()
+        self._ctx._check(lib.gfsm_plan_symmetry(self._h, C.byref(aut), C.byref(n), None))
+        cond = np.zeros(max(2 * n.value, 1), np.uint32)
+        self._ctx._check(lib.gfsm_plan_symmetry(self._h, None, None, cond.ctypes.data_as(_lib.u32p)))
+        return aut.value, [(int(cond[2 * i]), int(cond[2 * i + 1])) for i in range(n.value)]
+
     def info(self):
         """{"planner": 0 reference order / 1 data-aware, "order_invariant": bool}"""
         pl, inv = C.c_uint32(), C.c_uint32()

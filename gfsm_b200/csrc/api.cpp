@@ -286,6 +286,7 @@ gfsm_status gfsm_query_prepare(gfsm_ctx *ctx, const gfsm_graph *q, gfsm_plan **o
     auto p = std::make_unique<gfsm_plan>();
     gfsm_status rc = plan_query(q->h, q->rel_bits, p->p);
     if (rc != GFSM_OK) return set_err(ctx, rc, "");
+    plan_symmetry(q->h, p->p, ctx->lim.vertex_labels != 0);
     *out = p.release();
     return GFSM_OK;
 }
@@ -355,11 +356,13 @@ static std::vector<double> candidate_weights(const HostGraph &q, const Plan &p, 
 static gfsm_status plan_for(const HostGraph &q, uint32_t rel_bits, const PlanStats *st, const gfsm_limits &lim,
                             bool vl, Plan &out) {
     gfsm_status rc = plan_query(q, rel_bits, out);
-    if (rc != GFSM_OK || !st || !st->order_invariant || !out.order_invariant) return rc;
-    const std::vector<double> w = candidate_weights(q, out, *st, vl, lim.degree_filter != 0);
-    Plan alt;
-    if (plan_query(q, rel_bits, alt, &w) == GFSM_OK) out = std::move(alt);
-    return GFSM_OK;
+    if (rc == GFSM_OK && st && st->order_invariant && out.order_invariant) {
+        const std::vector<double> w = candidate_weights(q, out, *st, vl, lim.degree_filter != 0);
+        Plan alt;
+        if (plan_query(q, rel_bits, alt, &w) == GFSM_OK) out = std::move(alt);
+    }
+    if (rc == GFSM_OK) plan_symmetry(q, out, lim.vertex_labels != 0);
+    return rc;
 }
 
 gfsm_status gfsm_query_prepare_for(gfsm_ctx *ctx, const gfsm_graph *q, const gfsm_graph *data, gfsm_plan **out) {
@@ -377,6 +380,18 @@ gfsm_status gfsm_plan_info(const gfsm_plan *p, uint32_t *planner, uint32_t *orde
     if (!p) return GFSM_ERR_ARG;
     if (planner) *planner = p->p.planner;
     if (order_invariant) *order_invariant = p->p.order_invariant ? 1u : 0u;
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_plan_symmetry(const gfsm_plan *p, uint64_t *aut, uint32_t *n_cond, uint32_t *cond) {
+    if (!p) return GFSM_ERR_ARG;
+    if (aut) *aut = p->p.aut;
+    if (n_cond) *n_cond = (uint32_t)p->p.sym_cond.size();
+    if (cond)
+        for (size_t i = 0; i < p->p.sym_cond.size(); ++i) {
+            cond[2 * i] = p->p.sym_cond[i].first;
+            cond[2 * i + 1] = p->p.sym_cond[i].second;
+        }
     return GFSM_OK;
 }
 

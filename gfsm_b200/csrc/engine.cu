@@ -419,15 +419,30 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             const uint32_t na = L->next_anchor;
             const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
             const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-            uint32_t s = rs, e = re;  // the part of w's row inside depth+1's window
-            if (re - rs <= SHORT_ROW) {
+            // depth+1's window, narrowed by symmetry breaking: its candidate
+            // must exceed the vertices of next_lb and stay below those of next_ub
+            uint32_t klo = L->next_lo, khi = L->next_hi;
+            for (uint32_t m = L->next_lb; m; m &= m - 1u) {
+                const uint32_t pos = __ffs(m) - 1;
+                const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                klo = max(klo, x + 1);
+            }
+            for (uint32_t m = L->next_ub; m; m &= m - 1u) {
+                const uint32_t pos = __ffs(m) - 1;
+                const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+                khi = min(khi, x);
+            }
+            uint32_t s = rs, e = re;  // the part of w's row inside that window
+            if (klo >= khi) {
+                e = s;
+            } else if (re - rs <= SHORT_ROW) {
                 uint32_t b1, b2;
-                short_bounds(a.g.adj + rs, re - rs, L->next_lo, L->next_hi, b1, b2);
+                short_bounds(a.g.adj + rs, re - rs, klo, khi, b1, b2);
                 s = rs + b1;
                 e = rs + b2;
             } else {
-                if (L->next_lo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_lo);
-                if (L->next_hi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, L->next_hi);
+                if (klo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, klo);
+                if (khi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, khi);
             }
             if (e > s) {  // a child with no candidates cannot be extended: not written
                 emit = true;
@@ -841,7 +856,7 @@ inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 // Device plan of one query against one data graph
 // ---------------------------------------------------------------------------
 gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim, DQuery &dq,
-                         uint32_t &root_lo, uint32_t &root_hi, bool &never) {
+                         uint32_t &root_lo, uint32_t &root_hi, bool &never, bool sym) {
     std::memset(&dq, 0, sizeof(dq));
     never = false;
     const uint32_t k = p.k;
@@ -911,6 +926,17 @@ gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits 
         L.next_anchor = N.anchor;
         L.next_lo = N.lo;
         L.next_hi = N.hi;
+    }
+    if (sym) {
+        // f(a) < f(b): a bound on whichever of the two is placed later, taken
+        // from the earlier one's tuple position when its parent is written
+        std::vector<uint32_t> depth(k, 0);
+        for (uint32_t d = 0; d < k; ++d) depth[p.qvid[d]] = d;
+        for (const auto &c : p.sym_cond) {
+            const uint32_t da = depth[c.first], db = depth[c.second];
+            if (da < db) dq.lv[db - 1].next_lb |= (uint16_t)(1u << da);
+            else dq.lv[da - 1].next_ub |= (uint16_t)(1u << db);
+        }
     }
     root_lo = lo[0];
     root_hi = hi[0];
@@ -1167,6 +1193,13 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<int> active;
     std::vector<uint32_t> rlo, rhi;
     uint32_t dmax = 0;
+    // Symmetry breaking (a plan's aut > 1): exact where the count is the
+    // automorphism group's order times the count of one embedding per orbit
+    // -- symmetric data with one edge label and no repeated edge, counts
+    // only (mapping rows list every embedding); GFSM_SYMMETRY=0 turns it off.
+    const char *symv = getenv("GFSM_SYMMETRY");
+    const bool sym_ok = !rows_out && g.symmetric && !g.multi && g.elab == nullptr && !(symv && *symv == '0');
+    const bool vl_on = lim.vertex_labels != 0;
     {
         // independent per query: large batches use a few host threads
         std::vector<DQuery> all(nq);
@@ -1177,7 +1210,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         auto work = [&](int t) {
             for (int i = t; i < nq; i += nt) {
                 bool nv = false;
-                qrc[i] = build_dquery(*plans[i], g, lim, all[i], lo[i], hi[i], nv);
+                qrc[i] = build_dquery(*plans[i], g, lim, all[i], lo[i], hi[i], nv, sym_ok && plans[i]->aut > 1 &&
+                                                                                         plans[i]->sym_vl == vl_on);
                 never[i] = nv;
             }
         };
@@ -1366,9 +1400,14 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     ECHECK(cudaMemsetAsync(rows_ctr, 0, 4, stream));
     st.h2d_bytes += head_used;
     // per-query totals: every member of a final node gets its representative's count
+    // (times the automorphism group's order where symmetry breaking ran)
     auto gather_counts = [&](const std::vector<unsigned long long> &cnt) {
         std::vector<unsigned long long> out(na);
-        for (uint32_t i = 0; i < na; ++i) out[i] = cnt[final_rep[i]];
+        for (uint32_t i = 0; i < na; ++i) {
+            const Plan &pl = *plans[active[i]];
+            const bool sb = sym_ok && pl.aut > 1 && pl.sym_vl == vl_on;
+            out[i] = cnt[final_rep[i]] * (sb ? pl.aut : 1ull);
+        }
         return out;
     };
     ECHECK(cudaEventRecord(ev_begin, stream));

@@ -70,6 +70,14 @@ struct Plan {
     bool symmetric = false;          // query structure is symmetric
     bool order_invariant = false;    // symmetric with equal labels both ways, no repeated edge
     uint32_t planner = 0;            // 0: the reference's order; 1: data-aware order
+    // Symmetry breaking (order-invariant queries only): the query's
+    // automorphism group has `aut` elements; counting only the embeddings f
+    // with f(a) < f(b) for every (a, b) in sym_cond (query vertex ids) and
+    // multiplying by `aut` gives the full count.  sym_vl: automorphisms were
+    // required to keep vertex labels (vertex-label matching).
+    uint64_t aut = 1;
+    bool sym_vl = false;
+    std::vector<std::pair<uint32_t, uint32_t>> sym_cond;
 };
 
 // Per-depth device plan of one query against one data graph.
@@ -82,14 +90,14 @@ struct alignas(16) DLevel {
     uint8_t anchor_lab;        // label of the anchor requirement
     uint8_t final_;            // depth == k-1
     uint8_t anchor_check;      // anchor requirement needs a row search (multi-edge data)
-    uint8_t pad0, pad1;
+    uint16_t next_ub;          // symmetry breaking: depth+1's candidate < tuple[pos] for these positions
     uint8_t req_pos[MAXQ];     // tuple position, or REQ_SELF
     uint8_t req_lab[MAXQ];
     // shared-prefix trie (set on a node's representative): the node's child
     // nodes at depth+1 are fan_list[fan_start, fan_start + fan_count) when it
     // has more than one
     uint16_t fan_count;
-    uint16_t pad2;
+    uint16_t next_lb;          // symmetry breaking: depth+1's candidate > tuple[pos] for these positions
     uint32_t fan_start;
 };
 static_assert(sizeof(DLevel) == 64, "DLevel layout");
@@ -172,11 +180,17 @@ gfsm_status read_file(const char *path, std::string &out);
 // estimates query vertex v's data candidates and the order is data-aware
 // (only valid where the count cannot depend on the order).
 gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std::vector<double> *weight = nullptr);
+// Fills p.aut / p.sym_cond for an order-invariant query (labels kept when
+// vl).  Base points follow the matching order, so conditions bound later
+// depths by earlier ones.  Leaves aut = 1 if the search grows too large.
+void plan_symmetry(const HostGraph &q, Plan &p, bool vl);
 // builder.cu
 gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, DeviceGraph &out,
                                std::string &err);
 void free_device_graph(DeviceGraph &g);
 // engine.cu
+// sym: also encode the plan's symmetry-breaking conditions (the caller then
+// multiplies the count by p.aut).
 gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim,
-                         DQuery &dq, uint32_t &root_lo, uint32_t &root_hi, bool &never);
+                         DQuery &dq, uint32_t &root_lo, uint32_t &root_hi, bool &never, bool sym = false);
 }  // namespace gfsm

@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <thread>
 
 #include "gfsm_internal.h"
@@ -351,6 +352,94 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
     p.order_invariant = inv;
     p.planner = weight ? 1 : 0;
     return GFSM_OK;
+}
+
+// Symmetry breaking by a stabilizer chain (the conditions of Grochow and
+// Kellis): with base points b_0, b_1, ... and G_0 = Aut(Q), G_{i+1} the
+// stabilizer of b_i in G_i, the conditions f(b_i) < f(w) for every other w in
+// b_i's G_i-orbit keep exactly one embedding of each orbit of Aut(Q) acting
+// on embeddings (the action is free: embeddings are injective), and |Aut(Q)|
+// is the product of the orbit sizes.  Orbits are found by searching for one
+// automorphism per candidate image, never by listing the group.
+void plan_symmetry(const HostGraph &q, Plan &p, bool vl) {
+    p.aut = 1;
+    p.sym_vl = vl;
+    p.sym_cond.clear();
+    const uint32_t k = q.n;
+    if (!p.order_invariant || k < 2 || k > (uint32_t)MAXQ || p.qvid.size() != k) return;
+    // edge label of each ordered pair (0: no edge; labels are >= 1 here or
+    // the pair is absent), self-loops on the diagonal
+    std::vector<uint32_t> lab((size_t)k * k, 0);
+    for (size_t e = 0; e < q.src.size(); ++e) lab[(size_t)q.src[e] * k + q.dst[e]] = (uint32_t)q.lab[e] + 1u;
+    std::vector<uint32_t> deg(k, 0);
+    for (uint32_t a = 0; a < k; ++a)
+        for (uint32_t b = 0; b < k; ++b) deg[a] += lab[(size_t)a * k + b] != 0;
+    auto same_kind = [&](uint32_t a, uint32_t b) {
+        if (deg[a] != deg[b] || lab[(size_t)a * k + a] != lab[(size_t)b * k + b]) return false;
+        return !vl || (a < q.vlabel.size() ? q.vlabel[a] : 0) == (b < q.vlabel.size() ? q.vlabel[b] : 0);
+    };
+    uint64_t budget = 1u << 22;  // search nodes over the whole analysis
+    std::vector<int32_t> img(k), pre(k);
+    // is there an automorphism fixing base[0..nb) with a -> w?
+    std::function<bool(const std::vector<uint32_t> &, uint32_t)> extend;
+    std::vector<uint32_t> todo;
+    extend = [&](const std::vector<uint32_t> &seq, uint32_t i) -> bool {
+        if (i == seq.size()) return true;
+        if (budget == 0) return false;
+        --budget;
+        const uint32_t a = seq[i];
+        for (uint32_t w = 0; w < k; ++w) {
+            if (pre[w] >= 0 || !same_kind(a, w)) continue;
+            bool ok = true;
+            for (uint32_t j = 0; j < i && ok; ++j) {
+                const uint32_t x = seq[j], y = (uint32_t)img[x];
+                ok = lab[(size_t)a * k + x] == lab[(size_t)w * k + y] && lab[(size_t)x * k + a] == lab[(size_t)y * k + w];
+            }
+            if (!ok) continue;
+            img[a] = (int32_t)w;
+            pre[w] = (int32_t)a;
+            if (extend(seq, i + 1)) return true;
+            img[a] = -1;
+            pre[w] = -1;
+        }
+        return false;
+    };
+    auto exists = [&](const std::vector<uint32_t> &fixed, uint32_t a, uint32_t w) {
+        std::fill(img.begin(), img.end(), -1);
+        std::fill(pre.begin(), pre.end(), -1);
+        for (uint32_t x : fixed) img[x] = (int32_t)x, pre[x] = (int32_t)x;
+        if (pre[w] >= 0 || !same_kind(a, w)) return false;
+        for (uint32_t x : fixed)
+            if (lab[(size_t)a * k + x] != lab[(size_t)w * k + x] || lab[(size_t)x * k + a] != lab[(size_t)x * k + w])
+                return false;
+        img[a] = (int32_t)w;
+        pre[w] = (int32_t)a;
+        // the rest in matching order (neighbours of placed vertices first)
+        std::vector<uint32_t> seq(fixed);
+        seq.push_back(a);
+        for (uint32_t d = 0; d < k; ++d)
+            if (img[p.qvid[d]] < 0) seq.push_back(p.qvid[d]);
+        return extend(seq, (uint32_t)fixed.size() + 1);
+    };
+    std::vector<uint32_t> fixed;
+    uint64_t aut = 1;
+    std::vector<std::pair<uint32_t, uint32_t>> cond;
+    for (uint32_t d = 0; d < k; ++d) {
+        const uint32_t b = p.qvid[d];
+        uint64_t orbit = 1;
+        for (uint32_t w = 0; w < k; ++w) {
+            if (w == b || std::find(fixed.begin(), fixed.end(), w) != fixed.end()) continue;
+            if (exists(fixed, b, w)) {
+                ++orbit;
+                cond.push_back({b, w});
+            }
+            if (budget == 0) return;  // too large to analyse: no symmetry breaking
+        }
+        aut *= orbit;
+        fixed.push_back(b);
+    }
+    p.aut = aut;
+    p.sym_cond = std::move(cond);
 }
 
 }  // namespace gfsm

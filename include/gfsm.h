@@ -156,6 +156,16 @@ gfsm_status gfsm_query_prepare_for(gfsm_ctx *ctx, const gfsm_graph *query, const
 /* planner: 0 the reference's order, 1 data-aware; order_invariant: 1 if the
  * query's count cannot depend on the order.  Either pointer may be NULL. */
 gfsm_status gfsm_plan_info(const gfsm_plan *p, uint32_t *planner, uint32_t *order_invariant);
+/* Symmetry breaking of an order-invariant query: its automorphism group has
+ * *aut elements (keeping vertex labels when the context matches them), and
+ * counting only embeddings f with f(cond[2i]) < f(cond[2i+1]) for every
+ * i < *n_cond (query vertex ids, any fixed order of data vertices) and
+ * multiplying by *aut gives the full count -- which the matcher does for
+ * symmetric, single-edge-label data without repeated edges (not for mapping
+ * rows; GFSM_SYMMETRY=0 disables it).  No counterpart in the reference,
+ * which enumerates every automorphic image.  cond holds 2*(k-1)*k entries at
+ * most; any pointer may be NULL. */
+gfsm_status gfsm_plan_symmetry(const gfsm_plan *p, uint64_t *aut, uint32_t *n_cond, uint32_t *cond);
 /* gfsm_graph_from_edges + gfsm_query_prepare (data == NULL) or
  * gfsm_query_prepare_for (data given) for nq queries in one call, spread
  * over the host's threads.  No counterpart in the reference, which plans one

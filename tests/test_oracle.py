@@ -217,3 +217,39 @@ def test_data_aware_order_counts_the_same(tmp_path, vl):
             differ += mine.tables()["order"].tolist() != ref.tables()["order"].tolist()
     if vl:  # unlabelled, both orders take high-degree rows first and mostly agree
         assert differ > 0
+
+
+@pytest.mark.parametrize("vl", [False, True])
+def test_symmetry_breaking_counts_one_embedding_per_orbit(vl):
+    """gfsm_plan_symmetry: of every embedding the independent enumerator
+    lists, those meeting the conditions f(a) < f(b) (original vertex ids --
+    any fixed order works) number exactly total / |Aut(Q)|."""
+    import gfsm_b200
+    from gfsm_b200 import synth
+    ctx = gfsm_b200.GFSM(device=-1, vertex_labels=int(vl))
+    nontrivial = 0
+    for gi, g in enumerate([synth.er(60, 6.0, seed=5), synth.grid(9, 0.0, 0.1, seed=6),
+                            synth.ba(80, 3, seed=7)]):
+        g.vlabel = synth.vlabels(g.n, 2, 0.0, seed=8 + gi)
+        ds, dd = g.directed()
+        qs = [synth.rw_query(g, 3 + i % 4, tree=i % 2 == 0, seed=40 * gi + i)[0] for i in range(10)]
+        # plus small symmetric shapes: triangle, 4-cycle, star, 4-clique
+        shapes = [(3, [(0, 1), (1, 2), (2, 0)]), (4, [(0, 1), (1, 2), (2, 3), (3, 0)]),
+                  (4, [(0, 1), (0, 2), (0, 3)]), (4, [(a, b) for a in range(4) for b in range(a + 1, 4)])]
+        cases = [(q.n, *q.directed(), q.vlabel) for q in qs]
+        for n, ed in shapes:
+            s_ = np.array([a for a, b in ed] + [b for a, b in ed], np.uint32)
+            d_ = np.array([b for a, b in ed] + [a for a, b in ed], np.uint32)
+            cases.append((n, s_, d_, np.zeros(n, np.uint32)))
+        for n, qs_, qd_, qvl in cases:
+            plan = ctx.pre_process_query(ctx.graph_from_edges(n, qs_, qd_, None, qvl))
+            aut, cond = plan.symmetry()
+            total, rows = O.bt_count(n, qs_, qd_, None, qvl, g.n, ds, dd, None, g.vlabel, vlabel_mode=vl,
+                                     max_rows=1 << 22)
+            assert len(rows) == total
+            keep = np.ones(len(rows), bool)
+            for a, b in cond:
+                keep &= rows[:, a] < rows[:, b]
+            assert int(keep.sum()) * aut == total, (gi, n, aut, cond)
+            nontrivial += aut > 1
+    assert nontrivial >= 6
