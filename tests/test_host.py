@@ -196,3 +196,36 @@ def test_flat_batch_planning_and_plan_batch(host_ctx):
     assert batch[-1].tables()["k"] == qs[-1].n
     batch.close()
     assert len(batch) == 0
+
+
+def test_symmetry_group_orders_and_limits(host_ctx):
+    """|Aut(Q)| of known shapes (found without listing the group: K_16 has
+    16! elements), restricted by self-loops and edge labels; a directed query
+    (count depends on the order) gets none."""
+    import math
+    import time
+
+    def plan(n, edges, labels=None):
+        s = np.array([a for a, b in edges] + [b for a, b in edges if a != b], np.uint32)
+        d = np.array([b for a, b in edges] + [a for a, b in edges if a != b], np.uint32)
+        el = None if labels is None else np.array(list(labels) + [l for (a, b), l in zip(edges, labels) if a != b],
+                                                   np.uint32)
+        return host_ctx.pre_process_query(host_ctx.graph_from_edges(n, s, d, el, None))
+
+    t = time.perf_counter()
+    for n in (5, 8, 12, 16):
+        aut, cond = plan(n, [(a, b) for a in range(n) for b in range(a + 1, n)]).symmetry()
+        assert aut == math.factorial(n) and len(cond) == n * (n - 1) // 2
+    assert time.perf_counter() - t < 5.0
+    assert plan(6, [(i, (i + 1) % 6) for i in range(6)]).symmetry()[0] == 12       # C6: dihedral
+    assert plan(5, [(0, i) for i in range(1, 5)]).symmetry()[0] == 24              # K_{1,4}
+    assert plan(4, [(0, 1), (1, 2), (2, 3)]).symmetry()[0] == 2                    # path
+    # a self-loop on one end of a path breaks its reversal
+    assert plan(4, [(0, 1), (1, 2), (2, 3), (0, 0)]).symmetry()[0] == 1
+    # edge labels: a triangle with one edge of another label keeps one swap
+    assert plan(3, [(0, 1), (1, 2), (2, 0)], [1, 1, 2]).symmetry()[0] == 2
+    # an edge without its reverse: not order-invariant, no symmetry breaking
+    s = np.array([0, 1, 2, 1], np.uint32)
+    d = np.array([1, 2, 0, 0], np.uint32)
+    p = host_ctx.pre_process_query(host_ctx.graph_from_edges(3, s, d))
+    assert p.info()["order_invariant"] is False and p.symmetry() == (1, [])
