@@ -299,7 +299,7 @@ def run_ours(args, rank, world, local, pg):
 
     # -- device-resident batched steps
     clocks = Clocks(local)
-    dev_ms, k_ms, alg, launches, step_launches, cand = [], 0.0, 0, 0, 0, 0
+    dev_ms, k_ms, alg, launches, step_launches, cand, expans, embeds = [], 0.0, 0, 0, 0, 0, 0, 0
     barrier(pg)
     torch.cuda.synchronize(local)
     clocks.start()
@@ -312,6 +312,8 @@ def run_ours(args, rank, world, local, pg):
         alg += st["alg_bytes"]
         launches += st["launches"]          # every kernel of the call
         step_launches += st["steps"]        # level-step kernels
+        expans += st["expansions"]
+        embeds += int(counts.sum())
         cand += st["candidates"]
     torch.cuda.synchronize(local)
     barrier(pg)
@@ -446,6 +448,10 @@ def run_ours(args, rank, world, local, pg):
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "clocks": clk, "gpu_launches": launches, "ingest": ingest, "planner": planner,
+            "work": {"partial_mappings_per_s": expans / (sum(dev_ms) / 1000.0),
+                     "embeddings_per_s": embeds / (sum(dev_ms) / 1000.0),
+                     "candidates_per_s": cand / (sum(dev_ms) / 1000.0),
+                     "note": "device timeline of the timed batches; embeddings counted with exact counts"},
         }
         print(json.dumps(line), flush=True)
     ctx.close()
