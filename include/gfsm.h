@@ -11,8 +11,10 @@
  * Semantics (the reference's, kept bit-exact): non-induced, injective,
  * edge-label-checked subgraph matching where each query vertex is placed in
  * the reference's matching order and checked against the reference's
- * requirement table; every automorphic image counts; vertex labels are
- * ignored unless gfsm_limits.vertex_labels is set.
+ * requirement table; every automorphic image counts (on symmetric inputs the
+ * matcher enumerates one embedding per orbit of the query's automorphism
+ * group and multiplies, see gfsm_plan_symmetry -- the count is the same);
+ * vertex labels are ignored unless gfsm_limits.vertex_labels is set.
  */
 #ifndef GFSM_H
 #define GFSM_H
