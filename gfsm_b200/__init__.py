@@ -177,10 +177,7 @@ class PlanBatch:
 
     def close(self):
         if self._arr is not None:
-            destroy = self._ctx._lib.gfsm_plan_destroy
-            for h in self._arr:
-                if h:
-                    destroy(C.c_void_p(h))
+            self._ctx._lib.gfsm_plan_destroy_array(self._arr, self._n)
             self._arr = None
             self._n = 0
 

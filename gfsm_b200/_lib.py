@@ -35,6 +35,7 @@ SIGNATURES = {
     "gfsm_query_prepare_for": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "gfsm_plan_info": (C.c_int, [vp, u32p, u32p]),
     "gfsm_plan_symmetry": (C.c_int, [vp, u64p, u32p, u32p]),
+    "gfsm_plan_destroy_array": (None, [vp, C.c_int]),
     "gfsm_plan_tables": (C.c_int, [vp, u32p, u32p, u32p, u32p, u32p]),
     "gfsm_plan_columns": (C.c_int, [vp, u32p]),
     "gfsm_plan_destroy": (None, [vp]),

@@ -469,6 +469,11 @@ gfsm_status gfsm_plan_columns(const gfsm_plan *p, uint32_t *qvid) {
 
 void gfsm_plan_destroy(gfsm_plan *p) { delete p; }
 
+void gfsm_plan_destroy_array(gfsm_plan *const *plans, int n) {
+    if (!plans) return;
+    for (int i = 0; i < n; ++i) delete plans[i];
+}
+
 gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq, const gfsm_graph *data,
                              uint64_t *counts, gfsm_stats *stats) {
     if (!ctx || !data || nq < 0 || (nq && (!plans || !counts))) return GFSM_ERR_ARG;

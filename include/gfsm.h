@@ -190,6 +190,9 @@ gfsm_status gfsm_plan_tables(const gfsm_plan *p, uint32_t *k, uint32_t *max_vale
 /* Query vertex id (as in the query file) placed at each depth. */
 gfsm_status gfsm_plan_columns(const gfsm_plan *p, uint32_t *qvid);
 void        gfsm_plan_destroy(gfsm_plan *p);
+/* gfsm_plan_destroy for n plans at once (NULL entries are skipped), e.g. the
+ * output of gfsm_query_prepare_batch.  No counterpart in the reference. */
+void        gfsm_plan_destroy_array(gfsm_plan *const *plans, int n);
 
 /* --- matching ---------------------------------------------------------- */
 /* replaces HnSetup::solve / gpuLaunch (HnGPU.cu:710-1063): one query. */
