@@ -181,6 +181,20 @@ def peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
+def golden_counts(rank, nq):
+    """The oracle's counts for rank 0's batch (tests/golden/make_bench_counts.py),
+    or None when this batch is not the one recorded."""
+    if rank != 0:
+        return None
+    try:
+        rec = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_cfg5_counts.json")))
+    except Exception:
+        return None
+    if rec.get("workload") != WORKLOAD or len(rec["counts"]) < nq:
+        return None
+    return rec["counts"][:nq]
+
+
 def traffic_record():
     """Measured DRAM bytes per level-step launch from a committed ncu summary, if any."""
     try:
@@ -296,6 +310,13 @@ def run_ours(args, rank, world, local, pg):
     for _ in range(args.warmup):
         counts, st = ctx.batch_count(plans, data)
     ref_counts = counts.copy()
+    # every count of the batch against the oracle's (rank 0's batch is recorded)
+    gold = golden_counts(rank, args.queries)
+    exact_vs_oracle = None
+    if gold is not None:
+        agree = int(sum(int(a) == int(b) for a, b in zip(ref_counts.tolist(), gold)))
+        exact_vs_oracle = f"{agree}/{len(gold)}"
+        assert agree == len(gold), f"batched counts differ from the oracle's on {len(gold) - agree} queries"
 
     # -- device-resident batched steps
     clocks = Clocks(local)
@@ -443,7 +464,11 @@ def run_ours(args, rank, world, local, pg):
             "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": config_for(args.queries, world),
-            "exact": exact, "batched_over_plain": value / plain["queries_per_s"] if plain else None,
+            "exact": exact, "exact_vs_oracle": exact_vs_oracle,
+            "exact_note": "batched == plain == served on every query; every batched count equals the "
+                          "oracle's (tests/golden/bench_cfg5_counts.json, all queries); the CPU legs "
+                          "re-count their own samples",
+            "batched_over_plain": value / plain["queries_per_s"] if plain else None,
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},

@@ -1709,9 +1709,7 @@ constexpr uint32_t kNoAllocTiles = 65536;  // 64M candidates per step
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_ptr[kMaxDevices] = {};  // device address of the scratch, per device
+std::mutex g_noalloc_mu;  // serialises host threads; the array itself is one per device
 
 }  // namespace
 
@@ -1724,20 +1722,33 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     const gfsm_limits &lim = data->ctx->lim;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     *count = 0;
-    if (g.device < 0 || g.device >= kMaxDevices) return GFSM_ERR_ARG;
     if (cudaSetDevice(g.device) != cudaSuccess) return GFSM_ERR_CUDA;
 
-    // The host only knows the array by a stand-in symbol: resolve its device
-    // address once per device, with that device current.  This first call
-    // may load the module, so it belongs before any stream capture.
+    // The host only knows the array by a stand-in symbol: its device address
+    // is looked up on every call, with the data graph's device current (cheap
+    // once the module is loaded, and still right after a device reset has
+    // reloaded the module elsewhere).  The first call on a device may load
+    // the module, so it belongs before any stream capture.
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    unsigned char *scratch = g_noalloc_ptr[g.device];
-    if (!scratch) {
+    unsigned char *scratch = nullptr;
+    {
         void *addr = nullptr;
         if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return GFSM_ERR_CUDA;
         scratch = static_cast<unsigned char *>(addr);
-        g_noalloc_ptr[g.device] = scratch;
     }
+    // Once work is queued, a failing call waits for it before returning, so
+    // no copy or kernel of a failed call still touches the shared array when
+    // the next call starts.
+    bool queued = false;
+    auto fail = [&](gfsm_status s) {
+        if (queued) cudaStreamSynchronize(st);
+        cudaGetLastError();
+        return s;
+    };
+    const bool trace = [] {
+        const char *t = getenv("GFSM_TRACE");
+        return t && *t && *t != '0';
+    }();
 
     DQuery dq;
     uint32_t rlo = 0, rhi = 0;
@@ -1788,12 +1799,13 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
 
     // per-call inputs into the scratch; the count must start at zero
     const unsigned long long rc2[2] = {0ull, (unsigned long long)(rhi - rlo)};
+    queued = true;
     if (cudaMemcpyAsync(d_plan, &dq, sizeof(DQuery), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_rcoff, rc2, sizeof(rc2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_rcstart, &rlo, 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(d_count, 0, 8, st) != cudaSuccess || cudaMemsetAsync(d_root_rep, 0, 4, st) != cudaSuccess ||
         cudaMemsetAsync(rows_ctr, 0, 4, st) != cudaSuccess)
-        return GFSM_ERR_CUDA;
+        return fail(GFSM_ERR_CUDA);
 
     const uint64_t max_scan = std::min<uint64_t>(lim.max_scan_size, (uint64_t)kNoAllocTiles * TILE);
     GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
@@ -1803,6 +1815,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     total[0] = rc2[1];
     np[0] = 1;
     uint32_t d = 0;
+    unsigned long long candidates = 0;
     for (;;) {
         if (pos[d] >= total[d]) {
             if (d == 0) break;
@@ -1852,17 +1865,24 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(
             a.pcoff, a.np, a.c0, chunk, ntiles, TILE, tile_parent, tile_ctr, d_result, nullptr, 0);
         launch_step(0, d == 0, a, ntiles, st);
-        if (cudaGetLastError() != cudaSuccess) return GFSM_ERR_CUDA;
+        if (cudaGetLastError() != cudaSuccess) return fail(GFSM_ERR_CUDA);
         StepResult r;
         if (cudaMemcpyAsync(&r, d_result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
-            return GFSM_ERR_CUDA;
+            return fail(GFSM_ERR_CUDA);
         if (r.err) return GFSM_ERR_CUDA;
         if (emits && r.next_ovf && chunk <= TILE) return GFSM_ERR_TOO_LARGE;
-        if (emits && (r.n_children > buf[d].cap || r.next_ovf)) {
+        const bool retry = emits && (r.n_children > buf[d].cap || r.next_ovf);
+        if (trace)
+            fprintf(stderr, "gfsm-noalloc-step depth=%u cand=%llu children=%llu next=%llu tiles=%u retry=%d\n", d,
+                    chunk, emits ? r.n_children : 0ull, emits ? r.total_next : 0ull, ntiles, retry ? 1 : 0);
+        if (retry) {
             ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
             continue;
         }
+        // the candidate cap of the data graph's context, as gfsm_match_count applies it
+        candidates += chunk;
+        if (lim.max_candidates && candidates > lim.max_candidates) return GFSM_ERR_TOO_LARGE;
         pos[d] += chunk;
         if (emits) {
             ratio[d] = std::max(2.0 * (double)r.n_children / (double)chunk, ratio[d] * 0.5);
@@ -1877,7 +1897,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     unsigned long long c = 0;
     if (cudaMemcpyAsync(&c, d_count, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
-        return GFSM_ERR_CUDA;
+        return fail(GFSM_ERR_CUDA);
     *count = c;
     return GFSM_OK;
 }

@@ -213,12 +213,14 @@ gfsm_status gfsm_match_mappings(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm
  * array inside libgfsm.so (held on each device that loads the library until
  * the process exits); data's device CCSR must already exist
  * (gfsm_graph_to_device), and the work runs on `stream` (a cudaStream_t,
- * NULL = the default stream).  The first call on a device resolves the
- * array's device address and may load the module: make it before any stream
- * capture.  Every call shares the array, so calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialised.  A query
- * that cannot fit one tile of frontier per level in the array returns
- * GFSM_ERR_TOO_LARGE. */
+ * NULL = the default stream).  Every call looks up the array's device
+ * address; the first call on a device may load the module: make it before
+ * any stream capture.  Every call shares the array, so calls that overlap on
+ * the GPU (other streams, other host threads) race and must be serialised;
+ * a call that fails waits for its own queued work before it returns.  A
+ * query that cannot fit one tile of frontier per level in the array returns
+ * GFSM_ERR_TOO_LARGE, as does one that passes the candidate cap
+ * (max_candidates) of data's context. */
 gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfsm_graph *data, void *stream,
                                      uint64_t *count);
 /* Many queries against one resident data graph in one device pass. */

@@ -6,7 +6,9 @@ gfsm_match_count's exactly, on two calls in a row (the fixed scratch array
 keeps the previous call's contents), and device memory must not change
 between calls.  This file is collected last on purpose."""
 import ctypes as C
+import json
 import os
+import re
 
 import numpy as np
 import pytest
@@ -17,13 +19,19 @@ from gfsm_b200 import _lib, synth
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
+COUNTS = json.load(open(os.path.join(GOLD, "counts.json")))
+
+
+def _noalloc_rc(ctx, plan, data):
+    cnt = C.c_uint64()
+    rc = ctx._lib.gfsm_match_count_noalloc(plan.handle, data.handle, None, C.byref(cnt))
+    return rc, cnt.value
 
 
 def _noalloc(ctx, plan, data):
-    cnt = C.c_uint64()
-    rc = ctx._lib.gfsm_match_count_noalloc(plan.handle, data.handle, None, C.byref(cnt))
+    rc, cnt = _noalloc_rc(ctx, plan, data)
     assert rc == 0, gfsm_b200.GFSMError(rc)
-    return cnt.value
+    return cnt
 
 
 def test_noalloc_matches_match_count():
@@ -50,7 +58,10 @@ def test_noalloc_matches_match_count():
         qs, qd = qg.directed()
         cases.append((vctx, vctx.pre_process_query(vctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)), d3))
 
-    first = [_noalloc(c, p, d) for c, p, d in cases]  # first call on the device resolves the scratch
+    first = [_noalloc(c, p, d) for c, p, d in cases]  # the first call on the device may load the module
+    # the er200 cases are pinned by the golden counts (FFS restatement == enumerator)
+    for (qn, f) in zip(("_3_triangle", "_4_square", "_5_road5", "_5_plus"), first):
+        assert f == COUNTS[qn + "|er200"]["count"]
     for rep in range(2):
         for (c, p, d), f in zip(cases, first):
             want, _ = c.match_count(p, d)
@@ -75,4 +86,41 @@ def test_noalloc_requires_device_graph():
     p = ctx.pre_process_query(ctx.file_parse(os.path.join(GOLD, "queries", "_3_triangle.g")))
     cnt = C.c_uint64()
     assert ctx._lib.gfsm_match_count_noalloc(p.handle, d.handle, None, C.byref(cnt)) == 300
+    ctx.close()
+
+
+def test_noalloc_chunks_through_the_fixed_array(monkeypatch, capfd):
+    """A frontier far larger than one level's buffer (the context's
+    max_soln_size caps it at 2,048 partial mappings) must be cut into several
+    steps per level, with re-runs where a chunk overflowed, and still give
+    the golden count; GFSM_TRACE shows the steps."""
+    ctx = gfsm_b200.GFSM(device=0, max_soln_size=2048)
+    data = ctx.file_parse(os.path.join(GOLD, "data", "ba300.g")).to_device()
+    plan = ctx.pre_process_query(ctx.file_parse(os.path.join(GOLD, "queries", "_5_road5.g")))
+    monkeypatch.setenv("GFSM_TRACE", "1")
+    capfd.readouterr()
+    got = _noalloc(ctx, plan, data)
+    err = capfd.readouterr().err
+    monkeypatch.delenv("GFSM_TRACE")
+    assert got == COUNTS["_5_road5|ba300"]["count"]
+    steps = [dict(kv.split("=") for kv in line.split()[1:]) for line in err.splitlines()
+             if line.startswith("gfsm-noalloc-step")]
+    per_depth = {}
+    for st in steps:
+        per_depth[st["depth"]] = per_depth.get(st["depth"], 0) + 1
+    assert max(per_depth.values()) > 1, per_depth          # a level ran as several chunks
+    assert any(int(st["children"]) > 0 for st in steps)
+    assert _noalloc(ctx, plan, data) == got                # and again, on the array the last call left
+    ctx.close()
+
+
+def test_noalloc_candidate_cap_matches_match_count():
+    """The context's candidate cap stops both count paths with the same status."""
+    ctx = gfsm_b200.GFSM(device=0, max_candidates=5000)
+    data = ctx.file_parse(os.path.join(GOLD, "data", "ba300.g")).to_device()
+    plan = ctx.pre_process_query(ctx.file_parse(os.path.join(GOLD, "queries", "_5_road5.g")))
+    rc, _ = _noalloc_rc(ctx, plan, data)
+    with pytest.raises(gfsm_b200.GFSMError) as e:
+        ctx.match_count(plan, data)
+    assert rc == e.value.status != 0
     ctx.close()
