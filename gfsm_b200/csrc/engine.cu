@@ -124,7 +124,8 @@ struct StepArgs {
     const uint32_t *__restrict__ ptup;
     uint64_t pstride;
     const uint32_t *__restrict__ pcstart;
-    const unsigned long long *__restrict__ pcoff;  // [np+1]
+    unsigned long long *pcoff;                      // [np+1]; pcoff[np] = pcoff_end, written by the partition
+    unsigned long long pcoff_end;
     uint64_t np;
     const uint32_t *__restrict__ tile_parent;       // [ntiles+1]
     unsigned long long c0, cend;
@@ -154,8 +155,12 @@ constexpr uint32_t kBranch = 1u << 31;
 // Also zeroes the step's per-query count scratch: final-level counts of a
 // step are added to the totals only once the host accepts the step, so a step
 // re-run after a frontier overflow never counts twice.
-__global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_t np, unsigned long long c0,
-                            unsigned long long ncand, uint32_t ntiles, uint32_t tile_size,
+//
+// The parents' candidate prefix gets its closing entry here (coff[np] =
+// coff_end, the total the host took from the step that wrote the parents):
+// no tile of that step had to wait for the others to publish it.
+__global__ void k_partition(unsigned long long *coff, uint64_t np, unsigned long long coff_end,
+                            unsigned long long c0, unsigned long long ncand, uint32_t ntiles, uint32_t tile_size,
                             uint32_t *__restrict__ tile_parent, uint32_t *tile_ctr, StepResult *result,
                             unsigned long long *step_counts, uint32_t nq) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,6 +168,7 @@ __global__ void k_partition(const unsigned long long *__restrict__ coff, uint64_
     if (t == 0) {
         *tile_ctr = 0;
         *result = StepResult{};
+        coff[np] = coff_end;  // the searches below read coff[0, np) only
     }
     if (t > ntiles) return;
     const unsigned long long c = c0 + (t < ntiles ? (unsigned long long)t * tile_size : ncand - 1);
@@ -277,8 +283,9 @@ struct StepSmem {
 // Child slots of one tile (called by one thread): a single atomic on the
 // step's allocator takes agg_cnt consecutive slots and the matching range of
 // the next level's candidate prefix, so no tile waits for another.  Slot
-// order across tiles is the order of their atomics.  The tile that allocates
-// last publishes the step's totals and the prefix's closing entry.
+// order across tiles is the order of their atomics.  The step's totals are
+// the allocator word itself once the step has finished (the host, or the
+// schedule controller, reads them from there).
 __device__ __forceinline__ void tile_alloc(const StepArgs &a, const unsigned long long agg_cnt,
                                            const unsigned long long agg_deg, unsigned long long &ex_cnt,
                                            unsigned long long &ex_deg) {
@@ -289,15 +296,6 @@ __device__ __forceinline__ void tile_alloc(const StepArgs &a, const unsigned lon
     ex_cnt = old >> kAllocShift;
     ex_deg = old & kAllocMask;
     if (big || ex_deg + agg_deg > kAllocMask) atomicOr(&r->next_ovf, 1u);  // the host redoes a smaller chunk
-    __threadfence();  // this tile's allocation is visible before it counts as done
-    if (atomicAdd(&r->tiles_done, 1u) == a.ntiles - 1) {
-        __threadfence();
-        const unsigned long long tot = atomicAdd(&r->alloc, 0ull);
-        const unsigned long long n = tot >> kAllocShift, next = tot & kAllocMask;
-        r->n_children = n;
-        r->total_next = next;
-        if (n <= a.ccap) a.ccoff[n] = next;
-    }
 }
 
 // Per-tile context of the candidate check: the parents' candidate prefix
@@ -311,6 +309,54 @@ struct CandCtx {
     uint32_t req_stride;
     const uint32_t *rlo, *rhi, *rmode;
 };
+
+// The child a surviving candidate becomes: its own candidate slice for
+// depth+1 (r.cs, r.cnt; r.q gains kBranch when its trie node branches).
+// False when the slice is empty -- such a child cannot be extended and is
+// not written.
+__device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, Stage &r,
+                                           unsigned long long &my_bytes) {
+    const uint32_t p = r.p, v = r.v, q = r.q;
+    const DLevel *L = &a.plans[q].lv[d];
+    const uint32_t na = L->next_anchor;
+    const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
+    const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
+    // depth+1's window, narrowed by symmetry breaking: its candidate
+    // must exceed the vertices of next_lb and stay below those of next_ub
+    uint32_t klo = L->next_lo, khi = L->next_hi;
+    for (uint32_t m = L->next_lb; m; m &= m - 1u) {
+        const uint32_t pos = __ffs(m) - 1;
+        const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+        klo = max(klo, x + 1);
+    }
+    for (uint32_t m = L->next_ub; m; m &= m - 1u) {
+        const uint32_t pos = __ffs(m) - 1;
+        const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
+        khi = min(khi, x);
+    }
+    uint32_t s = rs, e = re;  // the part of w's row inside that window
+    if (klo >= khi) {
+        e = s;
+    } else if (re - rs <= SHORT_ROW) {
+        uint32_t b1, b2;
+        short_bounds(a.g.adj + rs, re - rs, klo, khi, b1, b2);
+        s = rs + b1;
+        e = rs + b2;
+    } else {
+        if (klo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, klo);
+        if (khi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, khi);
+    }
+    if (e <= s) return false;
+    // a branching node's child offers its slice to every child node
+    const uint32_t nf = L->fan_count;
+    const uint32_t mult = nf > 1 ? nf : 1u;
+    r.cs = s;
+    r.cnt = (e - s) * mult;
+    r.q = nf > 1 ? (q | kBranch) : q;
+    // the child's tuple and anchor row, read once per (member) parent
+    my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
+    return true;
+}
 
 // One candidate c of a level step: find its parent, check it (injectivity,
 // anchor label, remaining requirements), and either count it (last query
@@ -415,44 +461,10 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             fq = q;
             ++fc;
         } else {
-            // the child's own candidate slice for depth+1
-            const uint32_t na = L->next_anchor;
-            const uint32_t w = na == d ? v : __ldg(a.ptup + (uint64_t)(1 + na) * a.pstride + p);
-            const uint32_t rs = __ldg(a.g.rowptr + w), re = __ldg(a.g.rowptr + w + 1);
-            // depth+1's window, narrowed by symmetry breaking: its candidate
-            // must exceed the vertices of next_lb and stay below those of next_ub
-            uint32_t klo = L->next_lo, khi = L->next_hi;
-            for (uint32_t m = L->next_lb; m; m &= m - 1u) {
-                const uint32_t pos = __ffs(m) - 1;
-                const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                klo = max(klo, x + 1);
-            }
-            for (uint32_t m = L->next_ub; m; m &= m - 1u) {
-                const uint32_t pos = __ffs(m) - 1;
-                const uint32_t x = pos == d ? v : __ldg(a.ptup + (uint64_t)(1 + pos) * a.pstride + p);
-                khi = min(khi, x);
-            }
-            uint32_t s = rs, e = re;  // the part of w's row inside that window
-            if (klo >= khi) {
-                e = s;
-            } else if (re - rs <= SHORT_ROW) {
-                uint32_t b1, b2;
-                short_bounds(a.g.adj + rs, re - rs, klo, khi, b1, b2);
-                s = rs + b1;
-                e = rs + b2;
-            } else {
-                if (klo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, klo);
-                if (khi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, khi);
-            }
-            if (e > s) {  // a child with no candidates cannot be extended: not written
-                emit = true;
-                // a branching node's child offers its slice to every child node
-                const uint32_t nf = L->fan_count;
-                const uint32_t mult = nf > 1 ? nf : 1u;
-                rec = Stage{p, v, s, (e - s) * mult, nf > 1 ? (q | kBranch) : q};
-                // the child's tuple and anchor row, read once per (member) parent
-                my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
-            }
+            // the child's next-level slice is found in the tile's second
+            // pass, over the warp's survivors packed together
+            rec = Stage{p, v, 0, 0, q};
+            emit = true;
         }
     }
 }
@@ -528,8 +540,32 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             const uint32_t bal = __ballot_sync(0xffffffffu, emit);
             if (emit) wstage[wcnt + __popc(bal & ((1u << lane) - 1u))] = rec;
             wcnt += __popc(bal);
-            my_deg += emit ? rec.cnt : 0u;
         }
+    }
+    if (emits) {
+        // second pass over this warp's survivors, packed: each becomes a
+        // child with its next-level slice, or is dropped (empty slice); the
+        // kept ones move down in place (a round reads its entries before
+        // any is overwritten, and writes only at or below them).  Packed
+        // survivors keep all 32 lanes busy on the slice searches, and the
+        // first pass's state is dead by then (fewer live registers).
+        __syncwarp();
+        uint32_t kept = 0;
+        for (uint32_t e0 = 0; e0 < wcnt; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            Stage r{0, 0, 0, 0, 0};
+            bool keep = false;
+            if (e < wcnt) {
+                r = wstage[e];
+                keep = next_slice(a, d, r, my_bytes);
+            }
+            const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) wstage[kept + __popc(bal & ((1u << lane) - 1u))] = r;
+            kept += __popc(bal);
+            my_deg += keep ? r.cnt : 0u;
+            __syncwarp();
+        }
+        wcnt = kept;
     }
 
     // ---- final-depth counts: one shared add per warp in the common case
@@ -663,10 +699,11 @@ struct Ctl {
     uint32_t *cstart[MAXQ];
     unsigned long long *coff[MAXQ];
     StepArgs args;               // the step in flight (static fields preset by the host)
-    const unsigned long long *root_coff;
+    unsigned long long *root_coff;
     const uint32_t *root_cstart;
     unsigned long long *counts;        // per-entity totals (args.counts is the step scratch)
     uint32_t nq, accepted;
+    uint32_t tile;                     // candidates per tile of the graph's step kernel
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
     uint32_t d, dmax, emits, done, err;
@@ -689,7 +726,7 @@ __device__ void ctl_plan(Ctl &c) {
     if (chunk > c.max_scan) chunk = c.max_scan;
     if (emits) {
         const double allowed = (double)c.cap[d] / fmax((double)c.ratio[d], 1.0 / 8192.0);
-        const unsigned long long lim = (unsigned long long)fmax(allowed, (double)TILE);
+        const unsigned long long lim = (unsigned long long)fmax(allowed, (double)c.tile);
         if (chunk > lim) chunk = lim;
         if (chunk > kMaxEmitChunk) chunk = kMaxEmitChunk;
     }
@@ -707,9 +744,10 @@ __device__ void ctl_plan(Ctl &c) {
         a.pcoff = c.coff[d - 1];
     }
     a.np = c.np[d];
+    a.pcoff_end = c.total[d];
     a.c0 = c.pos[d];
     a.cend = c.pos[d] + chunk;
-    a.ntiles = (uint32_t)((chunk + TILE - 1) / TILE);
+    a.ntiles = (uint32_t)((chunk + c.tile - 1) / c.tile);
     if (emits) {
         a.ctup = c.tup[d];
         a.cstride = c.cap[d];
@@ -731,14 +769,15 @@ __device__ void ctl_plan(Ctl &c) {
 // Accounts the finished step (the host loop's logic).
 __device__ void ctl_after(Ctl &c) {
     const StepResult *rp = c.args.result;
-    const unsigned long long n = __ldcg(&rp->n_children), next = __ldcg(&rp->total_next);
+    const unsigned long long alloc = __ldcg(&rp->alloc);
+    const unsigned long long n = alloc >> kAllocShift, next = alloc & kAllocMask;
     const unsigned long long ab = __ldcg(&rp->alg_bytes);
     uint32_t e = __ldcg(&rp->err);
     const uint32_t ovf = __ldcg(&rp->next_ovf);
     const uint32_t d = c.d;
     c.steps++;
     c.accepted = 0;
-    if (c.emits && ovf && c.chunk <= TILE) e |= KERR_CAP;  // one tile's children alone overflow
+    if (c.emits && ovf && c.chunk <= c.tile) e |= KERR_CAP;  // one tile's children alone overflow
     if (e) {
         c.err |= e;
         c.done = 1;
@@ -802,14 +841,15 @@ __global__ void k_ctl(Ctl *ctl, cudaGraphConditionalHandle h, int first) {
 // fields are compile-time constant-bank operands like kernel parameters (a
 // runtime slot index turns every field read into a load: the R-MAT triangle
 // ran 10% slower that way).
-template <int SLOT>
+template <int SLOT, uint32_t TILE_SIZE>
 __global__ void k_part_g(const Ctl *ctl) {
     const StepArgs &a = c_args[SLOT];
     const unsigned long long ncand = a.cend - a.c0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ctl->nq; i += gridDim.x * blockDim.x)
         a.counts[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.pcoff[a.np] = a.pcoff_end;  // see k_partition
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= a.ntiles; t += gridDim.x * blockDim.x) {
-        const unsigned long long c = a.c0 + (t < a.ntiles ? (unsigned long long)t * TILE : ncand - 1);
+        const unsigned long long c = a.c0 + (t < a.ntiles ? (unsigned long long)t * TILE_SIZE : ncand - 1);
         uint64_t lo = 0, hi = a.np;
         while (hi - lo > 1) {
             const uint64_t mid = lo + ((hi - lo) >> 1);
@@ -820,10 +860,10 @@ __global__ void k_part_g(const Ctl *ctl) {
 }
 
 // Graph node: the level step on a fixed grid; every CTA takes tiles from the
-// step's tile queue.
-template <int SLOT>
-__global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g() {
-    __shared__ StepSmem<Geo0> sm;
+// step's tile queue.  One instantiation per argument slot and tile geometry.
+template <int SLOT, class G>
+__global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
+    __shared__ StepSmem<G> sm;
     __shared__ uint32_t s_tile[2];
     const StepArgs &a = c_args[SLOT];
     // the next tile is fetched while this one runs (double-buffered: a slot
@@ -834,18 +874,26 @@ __global__ void __launch_bounds__(Geo0::T, Geo0::MINB) k_step_g() {
     uint32_t tile = s_tile[0];
     for (uint32_t it = 1; tile < a.ntiles; ++it) {
         if (threadIdx.x == 0) s_tile[it & 1u] = atomicAdd(a.tile_ctr, 1u);
-        if (a.depth == 0) step_tile<true, Geo0>(a, tile, sm);
-        else step_tile<false, Geo0>(a, tile, sm);
+        if (a.depth == 0) step_tile<true, G>(a, tile, sm);
+        else step_tile<false, G>(a, tile, sm);
         __syncthreads();
         tile = s_tile[it & 1u];
     }
 }
 
+// Tile geometries the graph-driven schedule is instantiated for (the others
+// run the host-driven loop): graph_geo(variant) is the index into them, or
+// -1.
+constexpr int kGraphGeos = 2;
+constexpr int graph_geo(int variant) { return variant == 0 ? 0 : variant == 2 ? 1 : -1; }
+
 template <int... S>
-const void *slot_kernel(int s, bool step) {
-    static const void *part[] = {(const void *)k_part_g<S>...};
-    static const void *stepk[] = {(const void *)k_step_g<S>...};
-    return step ? stepk[s] : part[s];
+const void *slot_kernel(int s, int ggeo, bool step) {
+    static const void *part[kGraphGeos][sizeof...(S)] = {{(const void *)k_part_g<S, Geo0::TILE>...},
+                                                          {(const void *)k_part_g<S, Geo2::TILE>...}};
+    static const void *stepk[kGraphGeos][sizeof...(S)] = {{(const void *)k_step_g<S, Geo0>...},
+                                                           {(const void *)k_step_g<S, Geo2>...}};
+    return step ? stepk[ggeo][s] : part[ggeo][s];
 }
 
 inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
@@ -943,6 +991,27 @@ gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits 
     return GFSM_OK;
 }
 
+void root_partition(const uint32_t *rowptr, uint32_t lo, uint32_t hi, uint32_t nparts, uint64_t *bounds) {
+    const uint64_t n = hi > lo ? hi - lo : 0;
+    const uint64_t w = n ? (uint64_t)rowptr[hi] - rowptr[lo] : 0;
+    bounds[0] = 0;
+    for (uint32_t k = 1; k < nparts; ++k) {
+        if (w == 0) {  // no entries to balance: equal numbers of rows
+            bounds[k] = n * k / nparts;
+            continue;
+        }
+        // smallest x with rowptr[lo + x] - rowptr[lo] >= ceil(k * w / nparts)
+        const uint64_t target = (k * w + nparts - 1) / nparts;
+        uint64_t a = bounds[k - 1], b = n;
+        while (a < b) {
+            const uint64_t mid = a + (b - a) / 2;
+            if ((uint64_t)rowptr[lo + mid] - rowptr[lo] >= target) b = mid; else a = mid + 1;
+        }
+        bounds[k] = a;
+    }
+    bounds[nparts] = n;
+}
+
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
@@ -978,11 +1047,15 @@ void release_arg_slot(int s) {
 }
 }  // namespace
 
+static_assert(kGraphGeos == 2, "Engine keeps one graph per graph geometry");
+
 void Engine::release() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    if (graph) cudaGraphDestroy(graph);
-    graph_exec = nullptr;
-    graph = nullptr;
+    for (int i = 0; i < kGraphGeos; ++i) {
+        if (graph_exec[i]) cudaGraphExecDestroy(graph_exec[i]);
+        if (graph[i]) cudaGraphDestroy(graph[i]);
+        graph_exec[i] = nullptr;
+        graph[i] = nullptr;
+    }
     release_arg_slot(arg_slot);
     arg_slot = -1;
     if (arena) cudaFree(arena);
@@ -1031,10 +1104,12 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     ctl = p;
     arena_cap = arena_limit;
     {
-        int sms = 0, per_sm = 0;
+        int sms = 0, per_sm0 = 0, per_sm2 = 0;
         ECHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_g<0>, T, 0));
-        step_blocks = sms * std::max(per_sm, 1);
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, k_step_g<0, Geo0>, Geo0::T, 0));
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_step_g<0, Geo2>, Geo2::T, 0));
+        step_blocks[graph_geo(0)] = sms * std::max(per_sm0, 1);
+        step_blocks[graph_geo(2)] = sms * std::max(per_sm2, 1);
     }
     arg_slot = acquire_arg_slot();
     ECHECK(cudaStreamSynchronize(stream));
@@ -1056,13 +1131,20 @@ gfsm_status Engine::ensure_arena(uint64_t bytes, std::string &err) {
 // k_ctl(next step, cond) }.  Every pointer the nodes take is fixed for the
 // engine's lifetime (control block, constant slot), so the graph is built and
 // instantiated once and relaunched by every call.
-gfsm_status Engine::build_graph(std::string &err) {
-    if (graph_exec) return GFSM_OK;
-    if (arg_slot < 0 || graph_failed) return GFSM_ERR_CUDA;
+gfsm_status Engine::build_graph(int variant, std::string &err) {
+    const int gg = graph_geo(variant);
+    if (gg < 0) return GFSM_ERR_CUDA;
+    if (graph_exec[gg]) return GFSM_OK;
+    if (arg_slot < 0) {
+        last_graph_error = -2;  // every constant-memory argument slot is taken
+        return GFSM_ERR_CUDA;
+    }
+    if (graph_failed[gg]) return GFSM_ERR_CUDA;
     cudaGraph_t g = nullptr;
     auto fail = [&](cudaError_t e, const char *what) {
         if (g) cudaGraphDestroy(g);
-        graph_failed = true;
+        graph_failed[gg] = true;
+        last_graph_error = (int)e;
         cudaGetLastError();
         err = std::string(what) + ": " + cudaGetErrorString(e);
         return GFSM_ERR_CUDA;
@@ -1095,13 +1177,13 @@ gfsm_status Engine::build_graph(std::string &err) {
     if ((e = cudaGraphAddMemcpyNodeToSymbol(&b0, body, nullptr, 0, c_args, &cp->args, sizeof(StepArgs),
                                             (size_t)slot * sizeof(StepArgs), cudaMemcpyDeviceToDevice)) != cudaSuccess)
         return fail(e, "args copy node");
-    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, false));
-    kp.gridDim = dim3((unsigned)step_blocks);
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, false));
+    kp.gridDim = dim3((unsigned)step_blocks[gg]);
     kp.blockDim = dim3(256);
     kp.kernelParams = a_part;
     if ((e = cudaGraphAddKernelNode(&b1, body, &b0, 1, &kp)) != cudaSuccess) return fail(e, "partition node");
-    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, true));
-    kp.blockDim = dim3(T);
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, true));
+    kp.blockDim = dim3(gg == 0 ? Geo0::T : Geo2::T);
     kp.kernelParams = nullptr;
     if ((e = cudaGraphAddKernelNode(&b2, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "step node");
     kp.func = (void *)k_ctl;
@@ -1109,12 +1191,12 @@ gfsm_status Engine::build_graph(std::string &err) {
     kp.blockDim = dim3(256);
     kp.kernelParams = a_next;
     if ((e = cudaGraphAddKernelNode(&b3, body, &b2, 1, &kp)) != cudaSuccess) return fail(e, "ctl node");
-    if ((e = cudaGraphInstantiate(&graph_exec, g, 0)) != cudaSuccess) {
-        graph_exec = nullptr;
+    if ((e = cudaGraphInstantiate(&graph_exec[gg], g, 0)) != cudaSuccess) {
+        graph_exec[gg] = nullptr;
         return fail(e, "cudaGraphInstantiate");
     }
-    cudaGraphUpload(graph_exec, stream);  // its first launch does not pay the upload
-    graph = g;
+    cudaGraphUpload(graph_exec[gg], stream);  // its first launch does not pay the upload
+    graph[gg] = g;
     return GFSM_OK;
 }
 
@@ -1139,26 +1221,32 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
                          (uint64_t)std::lround(std::log2((double)plans.size() + 1.0));
     auto it = tuned.find(key);
     if (it != tuned.end()) return it->second;
-    const size_t ns = std::min<size_t>(plans.size(), 32);
-    std::vector<const Plan *> sample(plans.begin(), plans.begin() + ns);
-    std::vector<uint64_t> cnt(ns);
-    // Samples under 2 ms of device time are launch-bound and their timings
-    // mostly noise: keep the default there.  Elsewhere another geometry must
+    // The sample is the call's first 32 queries, grown fourfold (up to 2,048)
+    // while the default geometry takes under 2 ms on it: shorter samples are
+    // launch-bound and their timings mostly noise.  Another geometry must
     // beat the default by 2% to be chosen (repeat timings of a sample agree
     // within ~0.5%).
     int best = 0;
-    double base_ms = 0.0, best_ms = 1e300;
-    for (int v = 0; v < kVariants; ++v) {
-        gfsm_stats s{};
-        if (run(sample, g, lim, cnt.data(), &s, nullptr, 0, nullptr, err, v) != GFSM_OK) return 0;
-        if (v == 0) {
-            base_ms = s.device_ms;
-            if (base_ms < 2.0) break;
+    for (size_t ns = std::min<size_t>(plans.size(), 32);; ns = std::min<size_t>(plans.size(), ns * 4)) {
+        std::vector<const Plan *> sample(plans.begin(), plans.begin() + ns);
+        std::vector<uint64_t> cnt(ns);
+        gfsm_stats s0{};
+        if (run(sample, g, lim, cnt.data(), &s0, nullptr, 0, nullptr, err, 0) != GFSM_OK) return 0;
+        const double base_ms = s0.device_ms;
+        if (base_ms < 2.0) {
+            if (ns < plans.size() && ns < 2048) continue;
+            break;  // the whole call is short: keep the default
         }
-        if (s.device_ms < best_ms && (v == 0 || s.device_ms < 0.98 * base_ms)) {
-            best_ms = s.device_ms;
-            best = v;
+        double best_ms = base_ms;
+        for (int v = 1; v < kVariants; ++v) {
+            gfsm_stats sv{};
+            if (run(sample, g, lim, cnt.data(), &sv, nullptr, 0, nullptr, err, v) != GFSM_OK) return 0;
+            if (sv.device_ms < best_ms && sv.device_ms < 0.98 * base_ms) {
+                best_ms = sv.device_ms;
+                best = v;
+            }
         }
+        break;
     }
     tuned[key] = best;
     return best;
@@ -1166,7 +1254,8 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
 
 gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                         uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
-                        uint64_t *n_rows, std::string &err, int variant) {
+                        uint64_t *n_rows, std::string &err, int variant, uint32_t part, uint32_t nparts) {
+    if (nparts == 0 || part >= nparts || (nparts > 1 && rows_out)) return GFSM_ERR_ARG;
     // GFSM_TRACE=1: one line per step on stderr (depth, candidates, survivors,
     // kernel ms) -- the per-level frontier statistics of the reference's
     // pcsv_printf HnStep / HnPred lines (HnGPU.cu:431, 525)
@@ -1174,13 +1263,14 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         const char *t = getenv("GFSM_TRACE");
         return t && *t && *t != '0';
     }();
-    // Driver: GFSM_DRIVER=graph|host forces one.  By default a single query
-    // runs its whole schedule as one CUDA graph launch (no host round trip
-    // per step: plain p50 0.41 -> 0.33 ms on the grid workload) and a batch
-    // runs the host-driven loop with the autotuned tile geometry.
+    // Driver: GFSM_DRIVER=graph|host forces one.  By default the whole
+    // schedule runs as one CUDA graph launch (no host round trip per step:
+    // plain p50 0.41 -> 0.33 ms on the grid workload) wherever the tile
+    // geometry has a graph; a single query takes the default geometry, a
+    // batch the autotuned one.
     const char *drv = getenv("GFSM_DRIVER");
-    const bool want_graph = !trace && (drv && *drv ? !strcmp(drv, "graph") : plans.size() == 1);
-    if (variant < 0) variant = (plans.empty() || want_graph) ? 0 : pick_variant(plans, g, lim, err);
+    const bool want_graph = !trace && (drv && *drv ? !strcmp(drv, "graph") : true);
+    if (variant < 0) variant = (plans.size() <= 1) ? 0 : pick_variant(plans, g, lim, err);
     auto t_start = std::chrono::steady_clock::now();
     const int nq = (int)plans.size();
     gfsm_stats st{};
@@ -1220,9 +1310,16 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         work(0);
         for (auto &th : pool) th.join();
         dq.reserve(nq);
+        std::vector<uint64_t> cut(nparts + 1);
         for (int i = 0; i < nq; ++i) {
             if (qrc[i] != GFSM_OK) return qrc[i];
             if (never[i]) continue;
+            if (nparts > 1) {  // this part's share of the root window
+                root_partition(g.h_rowptr.data(), lo[i], hi[i], nparts, cut.data());
+                const uint32_t base = lo[i];
+                lo[i] = base + (uint32_t)cut[part];
+                hi[i] = base + (uint32_t)cut[part + 1];
+            }
             dq.push_back(all[i]);
             active.push_back(i);
             rlo.push_back(lo[i]);
@@ -1459,7 +1556,12 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }();
     // the graph-driven schedule (falls back to the host loop if the graph
     // cannot be built, e.g. when every constant-memory argument slot is taken)
-    const bool graph_driver = want_graph && build_graph(err) == GFSM_OK;
+    bool graph_driver = false;
+    if (want_graph && graph_geo(variant) >= 0) {
+        std::string gerr;
+        graph_driver = build_graph(variant, gerr) == GFSM_OK;
+        if (!graph_driver) st.graph_error = last_graph_error ? last_graph_error : -1;
+    }
     if (graph_driver) {
         Ctl c;
         std::memset(&c, 0, sizeof(c));
@@ -1479,6 +1581,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         c.max_scan = max_scan;
         c.max_candidates = lim.max_candidates;
         c.dmax = dmax;
+        c.tile = variant_tile(variant);
         StepArgs &a = c.args;
         a.g = gv;
         a.plans = d_plans;
@@ -1495,7 +1598,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         ECHECK(cudaMemcpyAsync(d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         st.h2d_bytes += sizeof(Ctl);
         ECHECK(cudaEventRecord(ev0, stream));
-        ECHECK(cudaGraphLaunch(graph_exec, stream));
+        ECHECK(cudaGraphLaunch(graph_exec[graph_geo(variant)], stream));
         ECHECK(cudaEventRecord(ev1, stream));
         ECHECK(cudaMemcpyAsync(&c, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
         std::vector<unsigned long long> ecnt(ne);
@@ -1513,6 +1616,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         st.alg_bytes = c.alg_bytes;
         st.kernel_ms = ms;
         st.device_ms = ms;
+        st.tile_variant = variant;
+        st.driver = 1;
         if (c.err) {
             err = "device schedule error bits " + std::to_string(c.err);
             if (stats) *stats = st;
@@ -1592,8 +1697,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_ctr = rows_ctr;
         a.root_rep = d_root_rep;
         a.fan_list = d_fan_list;
+        a.pcoff_end = total[d];
         k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, ne), 256), 256, 0, stream>>>(
-            a.pcoff, a.np, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts, ne);
+            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts,
+            ne);
         ECHECK(cudaEventRecord(ev0, stream));
         launch_step(variant, d == 0, a, ntiles, stream);
         ECHECK(cudaGetLastError());
@@ -1606,7 +1713,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         cudaEventElapsedTime(&ms, ev0, ev1);
         kms += ms;
         st.steps++;
-        const StepResult r = *h_result;
+        StepResult r = *h_result;
+        r.n_children = r.alloc >> kAllocShift;  // the step's totals are its allocator word
+        r.total_next = r.alloc & kAllocMask;
         if (r.err) {
             err = "device step error bits " + std::to_string(r.err);
             return GFSM_ERR_CUDA;
@@ -1862,14 +1971,17 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         a.root_rep = d_root_rep;
         // one query: a step either counts (last level) or emits, so a re-run
         // step never counts twice and the count goes straight to the total
+        a.pcoff_end = total[d];
         k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(
-            a.pcoff, a.np, a.c0, chunk, ntiles, TILE, tile_parent, tile_ctr, d_result, nullptr, 0);
+            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, TILE, tile_parent, tile_ctr, d_result, nullptr, 0);
         launch_step(0, d == 0, a, ntiles, st);
         if (cudaGetLastError() != cudaSuccess) return fail(GFSM_ERR_CUDA);
         StepResult r;
         if (cudaMemcpyAsync(&r, d_result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return fail(GFSM_ERR_CUDA);
+        r.n_children = r.alloc >> kAllocShift;  // the step's totals are its allocator word
+        r.total_next = r.alloc & kAllocMask;
         if (r.err) return GFSM_ERR_CUDA;
         if (emits && r.next_ovf && chunk <= TILE) return GFSM_ERR_TOO_LARGE;
         const bool retry = emits && (r.n_children > buf[d].cap || r.next_ovf);

@@ -31,10 +31,12 @@ struct Engine {
     // graph-driven schedule (one graph launch per call; built once per engine)
     int arg_slot = -1;             // constant-memory slot for this engine's step arguments
     void *ctl = nullptr;           // device control block (inside the small region)
-    int step_blocks = 0;           // fixed grid of the graph's step kernel
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    bool graph_failed = false;
+    // one graph per tile geometry the schedule is instantiated for (two)
+    int step_blocks[2] = {0, 0};   // fixed grid of the graph's step kernel
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    bool graph_failed[2] = {false, false};
+    int last_graph_error = 0;      // why the last graph could not be built (cudaError_t, or -2: no slot)
 
     Engine() = default;
     Engine(const Engine &) = delete;
@@ -43,13 +45,18 @@ struct Engine {
     void release();
     gfsm_status init(int dev, uint64_t arena_limit, uint64_t scan_limit, std::string &err);
     gfsm_status ensure_arena(uint64_t bytes, std::string &err);
-    gfsm_status build_graph(std::string &err);
+    // The graph-driven schedule for tile geometry `variant` (built once,
+    // relaunched by every call); GFSM_ERR_CUDA where there is none.
+    gfsm_status build_graph(int variant, std::string &err);
     // Counts every plan against g; counts_out[i] for plans[i].  With rows_out
     // (single plan only) also writes up to max_rows full mappings.
     // variant < 0: tile geometry chosen by the autotuner.
+    // part / nparts: count only the embeddings whose root lies in part
+    // `part` of each query's root window cut by root_partition (counts of
+    // the nparts parts add up to the whole count).
     gfsm_status run(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                     uint64_t *counts_out, gfsm_stats *stats, uint32_t *rows_out, uint64_t max_rows,
-                    uint64_t *n_rows, std::string &err, int variant = -1);
+                    uint64_t *n_rows, std::string &err, int variant = -1, uint32_t part = 0, uint32_t nparts = 1);
     int pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                      std::string &err);
     std::map<uint64_t, int> tuned;  // autotuner: workload class -> tile geometry

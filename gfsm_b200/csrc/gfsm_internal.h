@@ -43,6 +43,7 @@ struct DeviceGraph {
     uint8_t *elab = nullptr;          // [m], null when every entry has the same label
     uint32_t single_label = 0;        // the label when elab == null
     uint32_t *order = nullptr;        // [n] internal id -> original id
+    void *block = nullptr;            // the one allocation rowptr, adj, order and elab live in
     bool symmetric = false, multi = false;
     int n_edge_labels = 0;
     bool vl_grouped = false;
@@ -52,6 +53,10 @@ struct DeviceGraph {
     std::vector<uint32_t> group_value;// sorted distinct vertex label values (grouped mode)
     std::vector<uint32_t> group_start;// [groups+1]
     uint64_t bytes = 0;
+    // build time: allocation, host-to-device copies, device passes, copies
+    // back (CUDA events on the build stream), and the host wall time
+    double build_ms[4] = {0, 0, 0, 0};
+    double build_wall_ms = 0;
     uint32_t degree(uint32_t v) const { return h_rowptr[v + 1] - h_rowptr[v]; }
 };
 
@@ -111,7 +116,9 @@ struct alignas(16) DQuery {
 
 // Totals of one level step.  `alloc` hands out child slots: every tile adds
 // (its children << kAllocShift) + (their next-level candidates) with one
-// atomic, so slot order and the candidate prefix advance together.
+// atomic, so slot order and the candidate prefix advance together; once the
+// step has finished the word holds the step's totals, which the host copies
+// into n_children / total_next.
 struct StepResult {
     unsigned long long n_children;
     unsigned long long total_next;
@@ -119,7 +126,7 @@ struct StepResult {
     unsigned long long alloc;
     unsigned int err;          // error bits a kernel may raise (none does today; the host checks them)
     unsigned int rows;         // mapping rows claimed (mapping mode)
-    unsigned int tiles_done;   // tiles that have allocated (the last one publishes the totals)
+    unsigned int pad;
     unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
 };
 
@@ -193,4 +200,10 @@ void free_device_graph(DeviceGraph &g);
 // multiplies the count by p.aut).
 gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim,
                          DQuery &dq, uint32_t &root_lo, uint32_t &root_hi, bool &never, bool sym = false);
+// Degree-balanced cut of a root window [lo, hi) of internal ids into nparts
+// consecutive ranges: bounds[0..nparts] are offsets into the window, part k
+// is [lo + bounds[k], lo + bounds[k+1]), and each part's rows hold about
+// 1/nparts of the window's CCSR entries (a root's entries are its first
+// expansion).  rowptr is the CCSR row pointer over internal ids.
+void root_partition(const uint32_t *rowptr, uint32_t lo, uint32_t hi, uint32_t nparts, uint64_t *bounds);
 }  // namespace gfsm

@@ -157,7 +157,7 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         // the graph a single-query batch runs is built now, not on a request
         // (if no argument slot is left, the slot runs the host-driven loop)
         std::string gerr;
-        e->build_graph(gerr);
+        e->build_graph(0, gerr);
         // and the slot's frontier arena: a first request must not pay a
         // multi-GB cudaMalloc
         rc = e->ensure_arena(e->arena_cap, err);
