@@ -219,6 +219,18 @@ class Server:
             self._h = None
 
 
+def partition_rows(rowptr, lo, hi, nparts):
+    """gfsm_partition_rows: degree-balanced cut of CCSR rows [lo, hi) into
+    nparts consecutive parts (offsets into the window; host only)."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    b = np.zeros(nparts + 1, np.uint64)
+    rc = _lib.load().gfsm_partition_rows(rp.ctypes.data_as(_lib.u32p), int(lo), int(hi), int(nparts),
+                                         b.ctypes.data_as(_lib.u64p))
+    if rc:
+        raise GFSMError(rc)
+    return b
+
+
 class GFSM:
     """One device context (HnSetup::preinit, HnGPU.cu:847-862)."""
 
@@ -346,6 +358,27 @@ class GFSM:
         self._check(self._lib.gfsm_batch_count(self._h, arr, len(plans), data.handle,
                                                counts.ctypes.data_as(_lib.u64p), C.byref(st)))
         return counts[: len(plans)], st.as_dict()
+
+    def batch_count_part(self, plans, data, part, nparts):
+        """batch_count over part `part` of nparts of every query's root window
+        (gfsm_batch_count_part): the parts' counts add up to batch_count's."""
+        if isinstance(plans, PlanBatch):
+            arr = plans._arr
+        else:
+            arr = (C.c_void_p * max(len(plans), 1))(*[p.handle.value for p in plans])
+        counts = np.zeros(max(len(plans), 1), np.uint64)
+        st = Stats()
+        self._check(self._lib.gfsm_batch_count_part(self._h, arr, len(plans), data.handle, int(part), int(nparts),
+                                                    counts.ctypes.data_as(_lib.u64p), C.byref(st)))
+        return counts[: len(plans)], st.as_dict()
+
+    def root_partition(self, plan, data, nparts):
+        """(window_lo, bounds): the degree-balanced cut of plan's root window."""
+        b = np.zeros(nparts + 1, np.uint64)
+        lo = C.c_uint32()
+        self._check(self._lib.gfsm_root_partition(self._h, plan.handle, data.handle, int(nparts), C.byref(lo),
+                                                  b.ctypes.data_as(_lib.u64p)))
+        return lo.value, b
 
     def serve(self, data, **kw):
         return Server(self, data, **kw)

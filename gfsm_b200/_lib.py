@@ -43,6 +43,9 @@ SIGNATURES = {
     "gfsm_match_mappings": (C.c_int, [vp, vp, vp, u32p, C.c_uint64, u64p, u64p, vp]),
     "gfsm_batch_count": (C.c_int, [vp, C.POINTER(vp), C.c_int, vp, u64p, vp]),
     "gfsm_match_count_noalloc": (C.c_int, [vp, vp, vp, u64p]),
+    "gfsm_partition_rows": (C.c_int, [u32p, C.c_uint32, C.c_uint32, C.c_uint32, u64p]),
+    "gfsm_root_partition": (C.c_int, [vp, vp, vp, C.c_uint32, u32p, u64p]),
+    "gfsm_batch_count_part": (C.c_int, [vp, C.POINTER(vp), C.c_int, vp, C.c_uint32, C.c_uint32, u64p, vp]),
     "gfsm_serve_start": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "gfsm_serve_submit": (C.c_int, [vp, vp, C.c_uint64]),
     "gfsm_serve_poll": (C.c_int, [vp, vp, C.c_int, C.POINTER(C.c_int)]),
@@ -75,6 +78,11 @@ class GraphInfo(C.Structure):
         ("n_edge_labels", C.c_int32),
         ("on_device", C.c_int32),
         ("device_bytes", C.c_uint64),
+        ("build_alloc_ms", C.c_double),
+        ("build_h2d_ms", C.c_double),
+        ("build_kernel_ms", C.c_double),
+        ("build_d2h_ms", C.c_double),
+        ("build_wall_ms", C.c_double),
     ]
 
 
@@ -94,6 +102,8 @@ class Stats(C.Structure):
         ("d2h_bytes", C.c_uint64),
         ("tile_variant", C.c_int32),
         ("launches", C.c_uint32),
+        ("driver", C.c_int32),
+        ("graph_error", C.c_int32),
     ]
 
     def as_dict(self):

@@ -240,6 +240,11 @@ gfsm_status gfsm_graph_info_get(const gfsm_graph *g, gfsm_graph_info *info) {
         info->n_edge_labels = d.n_edge_labels;
         info->on_device = 1;
         info->device_bytes = d.bytes;
+        info->build_alloc_ms = d.build_ms[0];
+        info->build_h2d_ms = d.build_ms[1];
+        info->build_kernel_ms = d.build_ms[2];
+        info->build_d2h_ms = d.build_ms[3];
+        info->build_wall_ms = d.build_wall_ms;
     } else {
         std::vector<uint32_t> deg(g->h.n, 0);
         for (uint32_t s : g->h.src) deg[s]++;
@@ -490,6 +495,49 @@ gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int n
     }
     rc = e->run(ps, *data->dev, ctx->lim, counts, stats, nullptr, 0, nullptr, err);
     return set_err(ctx, rc, err);
+}
+
+gfsm_status gfsm_batch_count_part(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq, const gfsm_graph *data,
+                                  uint32_t part, uint32_t nparts, uint64_t *counts, gfsm_stats *stats) {
+    if (!ctx || !data || nq < 0 || (nq && (!plans || !counts)) || nparts == 0 || part >= nparts)
+        return GFSM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    gfsm_status rc = ensure_device(ctx, const_cast<gfsm_graph *>(data));
+    if (rc != GFSM_OK) return rc;
+    std::string err;
+    Engine *e = ctx_engine(ctx, *data->dev, rc, err);
+    if (!e) return set_err(ctx, rc, err);
+    std::vector<const Plan *> ps(nq);
+    for (int i = 0; i < nq; ++i) {
+        if (!plans[i]) return GFSM_ERR_ARG;
+        ps[i] = &plans[i]->p;
+    }
+    rc = e->run(ps, *data->dev, ctx->lim, counts, stats, nullptr, 0, nullptr, err, -1, part, nparts);
+    return set_err(ctx, rc, err);
+}
+
+gfsm_status gfsm_partition_rows(const uint32_t *rowptr, uint32_t lo, uint32_t hi, uint32_t nparts,
+                                uint64_t *bounds) {
+    if (!rowptr || !bounds || nparts == 0 || hi < lo) return GFSM_ERR_ARG;
+    root_partition(rowptr, lo, hi, nparts, bounds);
+    return GFSM_OK;
+}
+
+gfsm_status gfsm_root_partition(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data, uint32_t nparts,
+                                uint32_t *window_lo, uint64_t *bounds) {
+    if (!ctx || !plan || !data || !bounds || !window_lo || nparts == 0) return GFSM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    gfsm_status rc = ensure_device(ctx, const_cast<gfsm_graph *>(data));
+    if (rc != GFSM_OK) return rc;
+    DQuery dq;
+    uint32_t lo = 0, hi = 0;
+    bool never = false;
+    rc = build_dquery(plan->p, *data->dev, ctx->lim, dq, lo, hi, never);
+    if (rc != GFSM_OK) return set_err(ctx, rc, "query cannot be planned against this graph");
+    if (never) hi = lo;  // no root can match: an empty window
+    *window_lo = lo;
+    root_partition(data->dev->h_rowptr.data(), lo, hi, nparts, bounds);
+    return GFSM_OK;
 }
 
 gfsm_status gfsm_match_count(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data, uint64_t *count,

@@ -18,6 +18,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 
 #include "gfsm_internal.h"
@@ -106,14 +107,18 @@ inline unsigned grid_for(uint64_t n, unsigned threads) {
 }  // namespace
 
 void free_device_graph(DeviceGraph &g) {
-    if (g.rowptr) cudaFree(g.rowptr);
-    if (g.adj) cudaFree(g.adj);
-    if (g.elab) cudaFree(g.elab);
-    if (g.order) cudaFree(g.order);
+    if (g.block) cudaFree(g.block);
+    g.block = nullptr;
     g.rowptr = g.adj = g.order = nullptr;
     g.elab = nullptr;
 }
 
+// Host side of the build.  The outputs (rowptr, adj, order, elab) live in one
+// persistent allocation; every temporary (edge copies, keys, degrees, CUB
+// scratch) is carved from one stream-ordered workspace allocation released
+// with cudaFreeAsync, so the build holds no device-wide synchronisation
+// besides its final stream sync.  Events split the build into allocation,
+// host-to-device copies, device passes and the copies back.
 gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, DeviceGraph &out,
                                std::string &err) {
     gfsm_status rc = GFSM_OK;
@@ -128,19 +133,25 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
 
     uint32_t bits = 1;
     while ((1ull << bits) < (uint64_t)std::max<uint32_t>(n, 2)) ++bits;
+    const uint64_t n1 = std::max<uint32_t>(n, 1), m1 = std::max<uint64_t>(m, 1);
+    auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
 
-    uint32_t *d_src = nullptr, *d_dst = nullptr, *d_deg = nullptr, *d_group = nullptr;
-    uint32_t *d_inv = nullptr, *d_degs = nullptr, *d_val = nullptr, *d_order = nullptr, *d_flags = nullptr;
-    unsigned long long *d_vkey = nullptr, *d_vkey2 = nullptr, *d_ekey = nullptr, *d_ekey2 = nullptr;
-    uint8_t *d_lab = nullptr, *d_lab2 = nullptr;
-    void *d_tmp = nullptr;
-    size_t tmp_bytes = 0, need = 0;
+    char *ws = nullptr;
     uint32_t h_flags[3] = {0, 0, 0};
     std::vector<uint32_t> group;  // per vertex, when grouping by label
     cudaStream_t st = nullptr;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint32_t *d_src, *d_dst, *d_deg, *d_group, *d_inv, *d_degs, *d_val, *d_flags;
+    unsigned long long *d_vkey, *d_vkey2, *d_ekey, *d_ekey2;
+    uint8_t *d_lab, *d_lab2;
+    void *d_tmp;
+    size_t tmp_bytes = 0, need = 0;
+    int gbits = 0;
+    auto t_host0 = std::chrono::steady_clock::now();
 
     BCHECK(cudaSetDevice(device));
     BCHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : ev) BCHECK(cudaEventCreate(&e));
     if (vl_mode) {
         std::vector<uint32_t> vals(h.vlabel.begin(), h.vlabel.end());
         std::sort(vals.begin(), vals.end());
@@ -158,77 +169,114 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
         out.group_value = {0};
         out.group_start = {0, n};
     }
+    while ((1ull << gbits) < out.group_value.size()) ++gbits;
 
-    BCHECK(cudaMalloc(&d_src, std::max<uint64_t>(m, 1) * 4));
-    BCHECK(cudaMalloc(&d_dst, std::max<uint64_t>(m, 1) * 4));
-    BCHECK(cudaMalloc(&d_lab, std::max<uint64_t>(m, 1)));
-    BCHECK(cudaMalloc(&d_lab2, std::max<uint64_t>(m, 1)));
-    BCHECK(cudaMalloc(&d_deg, (uint64_t)std::max<uint32_t>(n, 1) * 4));
-    BCHECK(cudaMalloc(&d_flags, 16));
+    // scratch sizes of the CUB passes (queried with null pointers)
+    BCHECK(cub::DeviceRadixSort::SortPairs(nullptr, need, (unsigned long long *)nullptr,
+                                           (unsigned long long *)nullptr, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                           (int)n1, 0, 32 + gbits, st));
+    tmp_bytes = need;
+    BCHECK(cub::DeviceScan::ExclusiveSum(nullptr, need, (uint32_t *)nullptr, (uint32_t *)nullptr, (int)n1 + 1, st));
+    tmp_bytes = std::max(tmp_bytes, need);
+    BCHECK(cub::DeviceRadixSort::SortPairs(nullptr, need, (unsigned long long *)nullptr,
+                                           (unsigned long long *)nullptr, (uint8_t *)nullptr, (uint8_t *)nullptr,
+                                           (int64_t)m1, 0, 2 * bits, st));
+    tmp_bytes = std::max(tmp_bytes, need);
+
+    BCHECK(cudaEventRecord(ev[0], st));
+    {
+        // persistent outputs: rowptr | adj | order | elab
+        const uint64_t o_rowptr = 0, o_adj = al((n1 + 1) * 4), o_order = o_adj + al(m1 * 4),
+                       o_elab = o_order + al(n1 * 4), o_end = o_elab + al(m1);
+        BCHECK(cudaMalloc(&out.block, o_end));
+        char *b = static_cast<char *>(out.block);
+        out.rowptr = reinterpret_cast<uint32_t *>(b + o_rowptr);
+        out.adj = reinterpret_cast<uint32_t *>(b + o_adj);
+        out.order = reinterpret_cast<uint32_t *>(b + o_order);
+        d_lab2 = reinterpret_cast<uint8_t *>(b + o_elab);  // becomes out.elab when labels differ
+        // workspace
+        const uint64_t sizes[] = {m1 * 4, m1 * 4, m1, n1 * 4, n1 * 4, n1 * 4, (n1 + 1) * 4, n1 * 4, 64,
+                                  n1 * 8, n1 * 8, m1 * 8, m1 * 8, tmp_bytes};
+        uint64_t total = 0;
+        for (uint64_t x : sizes) total += al(x);
+        BCHECK(cudaMallocAsync(reinterpret_cast<void **>(&ws), total, st));
+        char *w = ws;
+        auto take = [&](uint64_t bytes) {
+            char *r = w;
+            w += al(bytes);
+            return r;
+        };
+        d_src = reinterpret_cast<uint32_t *>(take(sizes[0]));
+        d_dst = reinterpret_cast<uint32_t *>(take(sizes[1]));
+        d_lab = reinterpret_cast<uint8_t *>(take(sizes[2]));
+        d_deg = reinterpret_cast<uint32_t *>(take(sizes[3]));
+        d_group = reinterpret_cast<uint32_t *>(take(sizes[4]));
+        d_inv = reinterpret_cast<uint32_t *>(take(sizes[5]));
+        d_degs = reinterpret_cast<uint32_t *>(take(sizes[6]));
+        d_val = reinterpret_cast<uint32_t *>(take(sizes[7]));
+        d_flags = reinterpret_cast<uint32_t *>(take(sizes[8]));
+        d_vkey = reinterpret_cast<unsigned long long *>(take(sizes[9]));
+        d_vkey2 = reinterpret_cast<unsigned long long *>(take(sizes[10]));
+        d_ekey = reinterpret_cast<unsigned long long *>(take(sizes[11]));
+        d_ekey2 = reinterpret_cast<unsigned long long *>(take(sizes[12]));
+        d_tmp = take(sizes[13]);
+    }
+    BCHECK(cudaEventRecord(ev[1], st));
+
+    // 1. edges in, degree histogram
     if (m) {
         BCHECK(cudaMemcpyAsync(d_src, h.src.data(), m * 4, cudaMemcpyHostToDevice, st));
         BCHECK(cudaMemcpyAsync(d_dst, h.dst.data(), m * 4, cudaMemcpyHostToDevice, st));
         BCHECK(cudaMemcpyAsync(d_lab, h.lab.data(), m, cudaMemcpyHostToDevice, st));
     }
-    BCHECK(cudaMemsetAsync(d_deg, 0, (uint64_t)std::max<uint32_t>(n, 1) * 4, st));
+    if (vl_mode && n) BCHECK(cudaMemcpyAsync(d_group, group.data(), (uint64_t)n * 4, cudaMemcpyHostToDevice, st));
+    BCHECK(cudaEventRecord(ev[2], st));
+    BCHECK(cudaMemsetAsync(d_deg, 0, n1 * 4, st));
     BCHECK(cudaMemsetAsync(d_flags, 0, 16, st));
-    if (vl_mode && n) {
-        BCHECK(cudaMalloc(&d_group, (uint64_t)n * 4));
-        BCHECK(cudaMemcpyAsync(d_group, group.data(), (uint64_t)n * 4, cudaMemcpyHostToDevice, st));
-    }
     if (m) k_degree<<<grid_for(m, 256), 256, 0, st>>>(d_src, m, d_deg);
 
-    // 2. vertex order
-    BCHECK(cudaMalloc(&d_vkey, (uint64_t)std::max<uint32_t>(n, 1) * 8));
-    BCHECK(cudaMalloc(&d_vkey2, (uint64_t)std::max<uint32_t>(n, 1) * 8));
-    BCHECK(cudaMalloc(&d_val, (uint64_t)std::max<uint32_t>(n, 1) * 4));
-    BCHECK(cudaMalloc(&d_order, (uint64_t)std::max<uint32_t>(n, 1) * 4));
-    BCHECK(cudaMalloc(&d_inv, (uint64_t)std::max<uint32_t>(n, 1) * 4));
-    BCHECK(cudaMalloc(&d_degs, ((uint64_t)n + 1) * 4));
-    BCHECK(cudaMalloc(&out.rowptr, ((uint64_t)n + 1) * 4));
+    // 2. vertex order, 3. row pointers
     if (n) {
-        int gbits = 0;
-        while ((1ull << gbits) < out.group_value.size()) ++gbits;
-        k_vertex_keys<<<grid_for(n, 256), 256, 0, st>>>(d_deg, d_group, n, d_vkey, d_val);
-        BCHECK(cub::DeviceRadixSort::SortPairs(nullptr, need, d_vkey, d_vkey2, d_val, d_order, (int)n, 0,
+        k_vertex_keys<<<grid_for(n, 256), 256, 0, st>>>(d_deg, vl_mode ? d_group : nullptr, n, d_vkey, d_val);
+        BCHECK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_vkey, d_vkey2, d_val, out.order, (int)n, 0,
                                                32 + gbits, st));
-        tmp_bytes = need;
-        BCHECK(cub::DeviceScan::ExclusiveSum(nullptr, need, d_degs, out.rowptr, (int)n + 1, st));
-        tmp_bytes = std::max(tmp_bytes, need);
-        BCHECK(cub::DeviceRadixSort::SortPairs(nullptr, need, d_ekey, d_ekey2, d_lab, d_lab2,
-                                               (int64_t)std::max<uint64_t>(m, 1), 0, 2 * bits, st));
-        tmp_bytes = std::max(tmp_bytes, need);
-        BCHECK(cudaMalloc(&d_tmp, tmp_bytes));
-        BCHECK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_vkey, d_vkey2, d_val, d_order, (int)n, 0,
-                                               32 + gbits, st));
-        k_invert<<<grid_for(n, 256), 256, 0, st>>>(d_order, n, d_deg, d_inv, d_degs);
+        k_invert<<<grid_for(n, 256), 256, 0, st>>>(out.order, n, d_deg, d_inv, d_degs);
         BCHECK(cudaMemsetAsync(d_degs + n, 0, 4, st));
-        // 3. row pointers
         BCHECK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_degs, out.rowptr, (int)n + 1, st));
     } else {
         BCHECK(cudaMemsetAsync(out.rowptr, 0, 4, st));
     }
-    cudaFree(d_vkey); d_vkey = nullptr;
-    cudaFree(d_vkey2); d_vkey2 = nullptr;
-    cudaFree(d_val); d_val = nullptr;
 
     // 4. entries keyed (row(src), row(dst)), labels carried as values
-    BCHECK(cudaMalloc(&out.adj, std::max<uint64_t>(m, 1) * 4));
     if (m) {
-        BCHECK(cudaMalloc(&d_ekey, m * 8));
-        BCHECK(cudaMalloc(&d_ekey2, m * 8));
         k_edge_keys<<<grid_for(m, 256), 256, 0, st>>>(d_src, d_dst, m, d_inv, bits, d_ekey);
         BCHECK(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_ekey, d_ekey2, d_lab, d_lab2, (int64_t)m, 0,
                                                2 * bits, st));
         k_unpack<<<grid_for(m, 256), 256, 0, st>>>(d_ekey2, m, bits, out.adj, d_lab2, d_flags);
         k_symmetric<<<grid_for(m, 256), 256, 0, st>>>(d_ekey2, m, bits, out.rowptr, out.adj, d_flags);
     }
+    BCHECK(cudaGetLastError());
+    BCHECK(cudaEventRecord(ev[3], st));
     BCHECK(cudaMemcpyAsync(h_flags, d_flags, 12, cudaMemcpyDeviceToHost, st));
     out.h_rowptr.resize((uint64_t)n + 1);
     out.h_order.resize(n);
     BCHECK(cudaMemcpyAsync(out.h_rowptr.data(), out.rowptr, ((uint64_t)n + 1) * 4, cudaMemcpyDeviceToHost, st));
-    if (n) BCHECK(cudaMemcpyAsync(out.h_order.data(), d_order, (uint64_t)n * 4, cudaMemcpyDeviceToHost, st));
+    if (n) BCHECK(cudaMemcpyAsync(out.h_order.data(), out.order, (uint64_t)n * 4, cudaMemcpyDeviceToHost, st));
+    BCHECK(cudaEventRecord(ev[4], st));
+    BCHECK(cudaFreeAsync(ws, st));
+    ws = nullptr;
     BCHECK(cudaStreamSynchronize(st));
+    {
+        float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        cudaEventElapsedTime(&c, ev[2], ev[3]);
+        cudaEventElapsedTime(&d, ev[3], ev[4]);
+        out.build_ms[0] = a;
+        out.build_ms[1] = b;
+        out.build_ms[2] = c;
+        out.build_ms[3] = d;
+    }
     out.multi = h_flags[0] != 0;
     out.symmetric = m == 0 || h_flags[2] == 0;
     if (m == 0) {
@@ -240,13 +288,10 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
         out.n_edge_labels = 0;
         for (int i = 0; i < 256; ++i) out.n_edge_labels += seen[i];
         out.elab = d_lab2;
-        d_lab2 = nullptr;
     } else {
         out.n_edge_labels = 1;
         out.single_label = h.lab[0];
     }
-    out.order = d_order;
-    d_order = nullptr;
     out.rows = 0;
     out.max_degree = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -255,24 +300,15 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
         out.max_degree = std::max(out.max_degree, d);
     }
     out.bytes = ((uint64_t)n + 1) * 4 + m * 4 + (out.elab ? m : 0) + (uint64_t)n * 4;
+    out.build_wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
 
 done:
-    if (d_src) cudaFree(d_src);
-    if (d_dst) cudaFree(d_dst);
-    if (d_lab) cudaFree(d_lab);
-    if (d_lab2) cudaFree(d_lab2);
-    if (d_deg) cudaFree(d_deg);
-    if (d_group) cudaFree(d_group);
-    if (d_inv) cudaFree(d_inv);
-    if (d_degs) cudaFree(d_degs);
-    if (d_val) cudaFree(d_val);
-    if (d_order) cudaFree(d_order);
-    if (d_flags) cudaFree(d_flags);
-    if (d_vkey) cudaFree(d_vkey);
-    if (d_vkey2) cudaFree(d_vkey2);
-    if (d_ekey) cudaFree(d_ekey);
-    if (d_ekey2) cudaFree(d_ekey2);
-    if (d_tmp) cudaFree(d_tmp);
+    if (ws) {
+        cudaFreeAsync(ws, st);
+        cudaStreamSynchronize(st);
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
     if (rc != GFSM_OK) free_device_graph(out);
     return rc;

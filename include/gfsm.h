@@ -73,6 +73,9 @@ typedef struct {
     int32_t  n_edge_labels;/* distinct edge labels (after CCSRRelSize masking) */
     int32_t  on_device;    /* device CCSR built                                */
     uint64_t device_bytes;
+    /* device CCSR build (0 until built): allocation, host-to-device copies,
+     * device passes, copies back (CUDA events), and host wall time, ms */
+    double   build_alloc_ms, build_h2d_ms, build_kernel_ms, build_d2h_ms, build_wall_ms;
 } gfsm_graph_info;
 
 typedef struct {
@@ -90,6 +93,9 @@ typedef struct {
     uint64_t d2h_bytes;          /* device->host bytes copied by the call          */
     int32_t  tile_variant;       /* tile geometry the autotuner chose (0..3)        */
     uint32_t launches;           /* kernels the call launched (graph nodes included) */
+    int32_t  driver;             /* 1: the whole schedule ran as one CUDA graph launch;
+                                    0: the host-driven step loop                   */
+    int32_t  graph_error;        /* a graph was wanted but could not be built (cudaError_t) */
 } gfsm_stats;
 
 typedef struct {
@@ -226,6 +232,33 @@ gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfsm_graph *da
 /* Many queries against one resident data graph in one device pass. */
 gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq,
                              const gfsm_graph *data, uint64_t *counts, gfsm_stats *stats);
+
+/* --- root partition across GPUs ---------------------------------------- */
+/* No counterpart in the reference (its FFS runs on one GPU).  FFS subtrees
+ * under different root candidates are independent, so a query's count is
+ * the sum of counts over disjoint parts of its root window -- the data
+ * vertices its first query vertex may map to, in the order the first level
+ * step takes them.  One process per GPU, each with the data graph on its
+ * device, counts its own part; the parts' counts are summed (one 8-byte
+ * value per query: an all-reduce or a host sum).
+ *
+ * gfsm_partition_rows: the cut itself, host only.  [lo, hi) is a window of
+ * CCSR rows, rowptr the CCSR row pointer (rowptr[hi] valid); writes
+ * bounds[0..nparts], offsets into the window, so that part k =
+ * [lo + bounds[k], lo + bounds[k+1]) holds about 1/nparts of the window's
+ * entries (a root's entries are its first expansion). */
+gfsm_status gfsm_partition_rows(const uint32_t *rowptr, uint32_t lo, uint32_t hi, uint32_t nparts,
+                                uint64_t *bounds);
+/* The cut of plan's root window against data (built on the device first);
+ * *window_lo receives the window's first internal id. */
+gfsm_status gfsm_root_partition(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data, uint32_t nparts,
+                                uint32_t *window_lo, uint64_t *bounds);
+/* gfsm_batch_count restricted to part `part` (0 <= part < nparts) of every
+ * query's root window: summed over the nparts parts, the counts equal
+ * gfsm_batch_count's. */
+gfsm_status gfsm_batch_count_part(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq,
+                                  const gfsm_graph *data, uint32_t part, uint32_t nparts, uint64_t *counts,
+                                  gfsm_stats *stats);
 
 /* --- serving ------------------------------------------------------------ */
 gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_serve_config *cfg,

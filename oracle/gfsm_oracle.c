@@ -363,6 +363,7 @@ typedef struct {
     uint32_t *row_list;      /* data row offsets in CCSR order */
     uint32_t *row_vid;       /* row offset -> original vertex id (via a map) */
     uint32_t nrows;
+    uint32_t root_begin, root_end; /* roots taken: CCSR rows [root_begin, root_end) */
     uint32_t *qcol;          /* depth -> original query vertex id */
     uint32_t *qlab;          /* depth -> query vertex label */
     _Atomic uint64_t next_root;
@@ -440,8 +441,8 @@ static void *ffs_worker(void *arg)
     uint32_t m[64];
     uint64_t local = 0;
     for (;;) {
-        uint64_t i = atomic_fetch_add(&c->next_root, 1);
-        if (i >= c->nrows) break;
+        uint64_t i = c->root_begin + atomic_fetch_add(&c->next_root, 1);
+        if (i >= c->root_end) break;
         uint32_t r = c->row_list[i];
         int ok = 1;
         for (uint32_t j = 0; j < p->header[0] && ok; j++)                      /* hnInit :95-102 */
@@ -459,12 +460,21 @@ int orc_ffs_count(const orc_graph *q, const orc_plan_t *p, const orc_graph *d,
                   int vlabel_mode, int threads, uint64_t *count,
                   uint32_t *rows_out, uint64_t max_rows, uint64_t *n_rows)
 {
+    return orc_ffs_count_rows(q, p, d, vlabel_mode, threads, 0, 0xffffffffu, count, rows_out, max_rows, n_rows);
+}
+
+int orc_ffs_count_rows(const orc_graph *q, const orc_plan_t *p, const orc_graph *d,
+                       int vlabel_mode, int threads, uint32_t root_begin, uint32_t root_end, uint64_t *count,
+                       uint32_t *rows_out, uint64_t max_rows, uint64_t *n_rows)
+{
     if (p->err || q->err || d->err) return -1;
     if (p->k > 64) return -2;
     ffs_ctx c;
     memset(&c, 0, sizeof(c));
     c.q = q; c.d = d; c.p = p; c.vlabel_mode = vlabel_mode;
     c.nrows = d->rows;
+    c.root_end = root_end < d->rows ? root_end : d->rows;
+    c.root_begin = root_begin < c.root_end ? root_begin : c.root_end;
     c.row_list = malloc(sizeof(uint32_t) * (d->rows + 1));
     c.row_vid = malloc(sizeof(uint32_t) * (d->rows + 1));
     uint64_t off = 0;
@@ -725,13 +735,25 @@ int orc_bt_count(uint32_t qn, uint32_t qm, const uint32_t *qs, const uint32_t *q
 /* ------------------------------------------------------------------------- */
 typedef struct {
     uint32_t n; const uint64_t *ptr; const uint32_t *adj;
+    const uint32_t *vl; uint32_t nl;          /* vertex labels (NULL: no histogram) */
+    uint64_t *hist; pthread_mutex_t mu;       /* [nl^3] ordered label triples */
     _Atomic uint64_t next, total;
 } tri_ctx;
+
+static void tri_label_add(uint64_t *h, uint32_t nl, uint32_t a, uint32_t b, uint32_t c)
+{
+    /* the 6 orderings of the triangle's vertices (a 3-vertex triangle query
+     * maps onto every ordering once) */
+    h[(a * nl + b) * nl + c]++; h[(a * nl + c) * nl + b]++;
+    h[(b * nl + a) * nl + c]++; h[(b * nl + c) * nl + a]++;
+    h[(c * nl + a) * nl + b]++; h[(c * nl + b) * nl + a]++;
+}
 
 static void *tri_worker(void *arg)
 {
     tri_ctx *c = arg;
     uint64_t local = 0;
+    uint64_t *lh = c->vl ? calloc((uint64_t)c->nl * c->nl * c->nl, 8) : NULL;
     for (;;) {
         uint64_t x = atomic_fetch_add(&c->next, 64);
         if (x >= c->n) break;
@@ -743,16 +765,44 @@ static void *tri_worker(void *arg)
                 while (a < ae && b < be) {
                     if (c->adj[a] < c->adj[b]) a++;
                     else if (c->adj[a] > c->adj[b]) b++;
-                    else { local++; a++; b++; }
+                    else {
+                        local++;
+                        if (lh) tri_label_add(lh, c->nl, c->vl[x], c->vl[y], c->vl[c->adj[a]]);
+                        a++; b++;
+                    }
                 }
             }
         }
     }
     atomic_fetch_add(&c->total, local);
+    if (lh) {
+        pthread_mutex_lock(&c->mu);
+        for (uint64_t i = 0; i < (uint64_t)c->nl * c->nl * c->nl; i++) c->hist[i] += lh[i];
+        pthread_mutex_unlock(&c->mu);
+        free(lh);
+    }
     return NULL;
 }
 
+static int triangles_impl(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                          const uint32_t *vl, uint32_t nl, uint64_t *hist, int threads, uint64_t *count);
+
 int orc_triangles(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, int threads, uint64_t *count)
+{
+    return triangles_impl(n, m, src, dst, NULL, 0, NULL, threads, count);
+}
+
+int orc_triangle_label_hist(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                            const uint32_t *vlabel, uint32_t nl, int threads, uint64_t *hist, uint64_t *count)
+{
+    if (!vlabel || nl == 0 || nl > 64) return -1;
+    for (uint32_t v = 0; v < n; v++) if (vlabel[v] >= nl) return -2;
+    memset(hist, 0, 8ull * nl * nl * nl);
+    return triangles_impl(n, m, src, dst, vlabel, nl, hist, threads, count);
+}
+
+static int triangles_impl(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                          const uint32_t *vl, uint32_t nl, uint64_t *hist, int threads, uint64_t *count)
 {
     uint64_t *deg = calloc((uint64_t)n + 1, 8);
     for (uint64_t i = 0; i < m; i++) { deg[src[i]]++; deg[dst[i]]++; }
@@ -781,11 +831,14 @@ int orc_triangles(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *d
     }
     tri_ctx c; memset(&c, 0, sizeof(c));
     c.n = n; c.ptr = ptr; c.adj = adj;
+    c.vl = vl; c.nl = nl; c.hist = hist;
+    pthread_mutex_init(&c.mu, NULL);
     if (threads < 1) threads = 1;
     pthread_t *th = malloc(sizeof(pthread_t) * threads);
     for (int t = 0; t < threads; t++) pthread_create(&th[t], NULL, tri_worker, &c);
     for (int t = 0; t < threads; t++) pthread_join(th[t], NULL);
     *count = atomic_load(&c.total);
+    pthread_mutex_destroy(&c.mu);
     free(th); free(adj); free(fill); free(ptr); free(deg);
     return 0;
 }

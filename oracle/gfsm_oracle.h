@@ -86,6 +86,12 @@ void orc_pack_segments(const orc_graph *g, uint32_t rel_bits, uint32_t *out);
 int orc_ffs_count(const orc_graph *q, const orc_plan_t *p, const orc_graph *d,
                   int vlabel_mode, int threads, uint64_t *count,
                   uint32_t *rows_out, uint64_t max_rows, uint64_t *n_rows);
+/* orc_ffs_count over the roots in CCSR rows [root_begin, root_end) only (the
+ * rows the reference's hnInit takes in that order): the counts of
+ * consecutive row ranges add up to the whole count. */
+int orc_ffs_count_rows(const orc_graph *q, const orc_plan_t *p, const orc_graph *d,
+                       int vlabel_mode, int threads, uint32_t root_begin, uint32_t root_end, uint64_t *count,
+                       uint32_t *rows_out, uint64_t max_rows, uint64_t *n_rows);
 
 /* Independent backtracking enumerator over raw edge lists. */
 int orc_bt_count(uint32_t qn, uint32_t qm, const uint32_t *qs, const uint32_t *qd,
@@ -98,6 +104,12 @@ int orc_bt_count(uint32_t qn, uint32_t qm, const uint32_t *qs, const uint32_t *q
 /* Triangles of an undirected simple graph given as edges (u < v). */
 int orc_triangles(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst, int threads,
                   uint64_t *count);
+/* The same enumeration, histogrammed by vertex labels: hist[(a*nl + b)*nl + c]
+ * = embeddings of the 3-vertex triangle query whose vertices carry labels
+ * (a, b, c) in query order (each triangle counts once per ordering of its
+ * vertices); *count = triangles.  vlabel[v] < nl <= 64. */
+int orc_triangle_label_hist(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                            const uint32_t *vlabel, uint32_t nl, int threads, uint64_t *hist, uint64_t *count);
 
 #ifdef __cplusplus
 }

@@ -56,11 +56,16 @@ def load():
         lib.orc_pack_segments.argtypes = [C.POINTER(OrcGraph), C.c_uint32, u32p]
         lib.orc_ffs_count.argtypes = [C.POINTER(OrcGraph), C.POINTER(OrcPlan), C.POINTER(OrcGraph), C.c_int,
                                       C.c_int, u64p, u32p, C.c_uint64, u64p]
+        lib.orc_ffs_count_rows.argtypes = [C.POINTER(OrcGraph), C.POINTER(OrcPlan), C.POINTER(OrcGraph), C.c_int,
+                                           C.c_int, C.c_uint32, C.c_uint32, u64p, u32p, C.c_uint64, u64p]
         lib.orc_bt_count.argtypes = [C.c_uint32, C.c_uint32, u32p, u32p, u32p, u32p,
                                      C.c_uint32, C.c_uint64, u32p, u32p, u32p, u32p,
                                      C.c_uint32, C.c_int, C.c_int, u64p, u32p, C.c_uint64, u64p]
         lib.orc_triangles.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int, u64p]
-        for f in ("orc_parse_file", "orc_parse_buffer", "orc_plan", "orc_ffs_count", "orc_bt_count",
+        lib.orc_triangle_label_hist.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, u32p, C.c_uint32, C.c_int,
+                                                u64p, u64p]
+        for f in ("orc_parse_file", "orc_parse_buffer", "orc_plan", "orc_ffs_count", "orc_ffs_count_rows", "orc_bt_count",
+                  "orc_triangle_label_hist",
                   "orc_triangles"):
             getattr(lib, f).restype = C.c_int
         _lib = lib
@@ -170,6 +175,26 @@ def ffs_count(q, plan, d, vlabel_mode=False, threads=1, max_rows=0):
     return cnt.value
 
 
+def ffs_count_rows(q, plan, d, root_begin, root_end, vlabel_mode=False, threads=1):
+    """ffs_count over the roots in CCSR rows [root_begin, root_end) only."""
+    cnt = C.c_uint64()
+    rc = load().orc_ffs_count_rows(C.byref(q._g), C.byref(plan._p), C.byref(d._g), int(vlabel_mode), int(threads),
+                                   int(root_begin), int(root_end), C.byref(cnt), None, 0, None)
+    if rc:
+        raise RuntimeError(f"orc_ffs_count_rows failed ({rc})")
+    return cnt.value
+
+
+def row_degrees(d):
+    """Out-degree of every CCSR row of an oracle Graph, in row order."""
+    seg = d.arrays()["seg_val"]
+    out, off = [], 0
+    while off < len(seg):
+        out.append(int(seg[off]))
+        off += int(seg[off]) + 1
+    return np.array(out, np.uint32)
+
+
 def bt_count(qn, qsrc, qdst, qlab, qvl, dn, dsrc, dst, dlab, dvl, rel_bits=8, vlabel_mode=False, threads=1,
              max_rows=0):
     """Independent backtracking enumerator over directed edge lists."""
@@ -200,6 +225,43 @@ def triangles(n, src, dst, threads=8):
     cnt = C.c_uint64()
     load().orc_triangles(int(n), len(s), s.ctypes.data_as(u32p), d.ctypes.data_as(u32p), int(threads), C.byref(cnt))
     return cnt.value
+
+
+def triangle_label_hist(n, src, dst, vlabel, nl, threads=8):
+    """hist[a, b, c]: embeddings of the triangle query with vertex labels
+    (a, b, c) in an undirected simple graph (edges src[i] < dst[i])."""
+    s = np.ascontiguousarray(src, np.uint32)
+    d = np.ascontiguousarray(dst, np.uint32)
+    vl = np.ascontiguousarray(vlabel, np.uint32)
+    h = np.zeros(nl ** 3, np.uint64)
+    cnt = C.c_uint64()
+    rc = load().orc_triangle_label_hist(int(n), len(s), s.ctypes.data_as(u32p), d.ctypes.data_as(u32p),
+                                        vl.ctypes.data_as(u32p), int(nl), int(threads), h.ctypes.data_as(u64p),
+                                        C.byref(cnt))
+    if rc:
+        raise RuntimeError(f"orc_triangle_label_hist failed ({rc})")
+    return h.reshape(nl, nl, nl)
+
+
+def path3_label_counts(n, src, dst, vlabel, nl):
+    """cnt[a, b, c]: embeddings of the 3-vertex path query x-y-z with vertex
+    labels (a, b, c) in an undirected simple graph, by the closed form
+    sum over y with label b of N_a(y) N_c(y) - [a == c] N_a(y), N_l(y) being
+    y's neighbours with label l (x != z is the only injectivity constraint
+    left: x, z are neighbours of y, so they differ from y)."""
+    vl = np.asarray(vlabel, np.int64)
+    s = np.asarray(src, np.int64)
+    d = np.asarray(dst, np.int64)
+    nb = np.zeros((n, nl), np.int64)          # N_l(y)
+    np.add.at(nb, (s, vl[d]), 1)
+    np.add.at(nb, (d, vl[s]), 1)
+    out = np.zeros((nl, nl, nl), np.int64)
+    for b in range(nl):
+        rows = nb[vl == b]
+        prod = rows.T @ rows                   # [a, c] = sum N_a N_c
+        prod[np.diag_indices(nl)] -= rows.sum(axis=0)
+        out[:, b, :] = prod
+    return out
 
 
 def ref_frontend_dump(path, plan=False):

@@ -251,10 +251,13 @@ def test_triangles_medium_rmat(gpu_ctx):
     assert gpu_ctx.solve(tri, data) == 6 * O.triangles(g.n, g.src, g.dst)
 
 
-def test_device_and_host_drivers_agree(monkeypatch):
+@pytest.mark.parametrize("tile", ["0", "2"])
+def test_device_and_host_drivers_agree(monkeypatch, tile):
     """The graph-driven schedule (one CUDA graph launch, decisions on the
     device) and the host-driven step loop make the same decisions: identical
-    counts, candidates and expansions."""
+    counts, candidates and expansions, for both tile geometries the graph is
+    instantiated for."""
+    monkeypatch.setenv("GFSM_TILE", tile)
     ctx = gfsm_b200.GFSM(device=0, vertex_labels=1, mem_limit=256 << 20)
     g = synth.grid(300, 0.05, 0.02, seed=8)
     g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=9)
@@ -278,6 +281,8 @@ def test_device_and_host_drivers_agree(monkeypatch):
     # host loop; the graph's controller, partition, step and controller nodes
     assert 2 * host_st["steps"] <= host_st["launches"] <= 3 * host_st["steps"]
     assert dev_st["launches"] == 1 + 3 * dev_st["steps"]
+    assert (host_st["driver"], dev_st["driver"]) == (0, 1)
+    assert dev_st["tile_variant"] == int(tile) and dev_st["graph_error"] == 0
     for (c1, s1), (c2, s2) in zip(host_single, dev_single):
         assert c1 == c2 and s1["candidates"] == s2["candidates"]
     assert host_st["steps"] > 20

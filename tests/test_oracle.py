@@ -270,3 +270,23 @@ def test_config1_ffs_matches_backtracking(vl, tmp_path):
     qs, qd = q.directed()
     bt = O.bt_count(q.n, qs, qd, None, q.vlabel, g.n, ds, dd, None, g.vlabel, vlabel_mode=vl, threads=8)
     assert ffs == bt > 0
+
+
+def test_three_vertex_closed_forms_match_backtracking():
+    """The exact methods the large-configuration fixtures use for 3-vertex
+    queries -- the labelled 2-path closed form and the labelled triangle
+    histogram -- equal the independent enumerator on every label pattern."""
+    g = synth.er(300, 6.0, seed=3)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=4)
+    H = O.triangle_label_hist(g.n, g.src, g.dst, g.vlabel, 3)
+    P = O.path3_label_counts(g.n, g.src, g.dst, g.vlabel, 3)
+    ds, dd = g.directed()
+    tri = (np.array([0, 1, 0, 1, 2, 2], np.uint32), np.array([1, 0, 2, 2, 0, 1], np.uint32))
+    path = (np.array([0, 1, 1, 2], np.uint32), np.array([1, 0, 2, 1], np.uint32))
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                qvl = np.array([a, b, c], np.uint32)
+                assert O.bt_count(3, *tri, None, qvl, g.n, ds, dd, None, g.vlabel, vlabel_mode=True) == H[a, b, c]
+                assert O.bt_count(3, *path, None, qvl, g.n, ds, dd, None, g.vlabel, vlabel_mode=True) == P[a, b, c]
+    assert H.sum() == 6 * O.triangles(g.n, g.src, g.dst)
