@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip the one-at-a-time measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-planner", action="store_true", help="skip the data-aware-order measurement")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference-build comparison")
+    ap.add_argument("--no-configs", action="store_true", help="skip the configuration 2 / 4 legs")
     return ap.parse_args()
 
 
@@ -234,6 +236,195 @@ class CpuOracle:
         return done, time.perf_counter() - t0, counts
 
 
+def ref_gpu_leg(g, qs, local):
+    """The reference GFSM build on this GPU (baseline/_ref/ref_gpu: the
+    reference's own parser, planner and level kernels, its level driver
+    restated on the host) beside this build, on the first 64 queries of the
+    batch with at most 5 vertices, vertex labels ignored -- the reference's
+    semantics, in which 6+-vertex queries overflow its 500M-record buffers.
+    Every count is checked against the oracle's
+    (tests/golden/bench_cfg5_refsubset_counts.json)."""
+    import tempfile
+
+    import gfsm_b200
+    exe = os.path.join(ROOT, "baseline", "_ref", "ref_gpu")
+    try:
+        gold = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_cfg5_refsubset_counts.json")))
+    except Exception:
+        return {"unavailable": "tests/golden/bench_cfg5_refsubset_counts.json missing"}
+    idx = gold["indices"]
+    if gold.get("workload") != WORKLOAD or max(idx) >= len(qs):
+        return {"unavailable": "the recorded subset is not this batch"}
+    sub = [qs[i] for i in idx]
+    want = gold["counts"]
+    out = {"queries": len(sub), "subset": gold["subset"], "vertex_labels": False}
+    # -- this build, vertex labels ignored
+    ctx0 = gfsm_b200.GFSM(device=local)
+    s, d = g.directed()
+    data0 = ctx0.graph_from_edges(g.n, s, d).to_device()
+    plans0 = ctx0.prepare_queries([(q.n,) + tuple(q.directed()) + (None, None) for q in sub])
+    for p in plans0:  # warm-up: engine arena, module, tuning
+        ctx0.match_count(p, data0)
+    lat, dev, got = [], [], []
+    for p in plans0:
+        t0 = time.perf_counter()
+        c, st = ctx0.match_count(p, data0)
+        lat.append((time.perf_counter() - t0) * 1000.0)
+        dev.append(st["device_ms"])
+        got.append(c)
+    ctx0.batch_count(plans0, data0)
+    t0 = time.perf_counter()
+    bcounts, bst = ctx0.batch_count(plans0, data0)
+    b_wall = (time.perf_counter() - t0) * 1000.0
+    out["ours_plain"] = {"queries_per_s": len(sub) / (sum(lat) / 1000.0), "ms_per_query_mean": float(np.mean(lat)),
+                         "device_ms_per_query_mean": float(np.mean(dev)),
+                         "exact_vs_oracle": got == want}
+    out["ours_batched"] = {"queries_per_s": len(sub) / (b_wall / 1000.0), "batch_wall_ms": b_wall,
+                           "batch_device_ms": bst["device_ms"], "exact_vs_oracle": bcounts.tolist() == want}
+    plans0.close()
+    ctx0.close()
+    if not os.path.exists(exe):
+        out["reference"] = {"unavailable": "baseline/_ref/ref_gpu not built (make -C baseline REFDIR=<reference>)"}
+        return out
+    # -- the reference build: one process, the data graph parsed and copied once
+    tmp = tempfile.mkdtemp()
+    dpath = os.path.join(tmp, "d.g")
+    g.write_text(dpath)
+    qpaths = []
+    for i, q in enumerate(sub):
+        qp = os.path.join(tmp, f"q{i}.g")
+        q.write_text(qp)
+        qpaths.append(qp)
+    res_path = os.path.join(tmp, "ref.jsonl")
+    r = subprocess.run([exe, dpath, res_path] + qpaths, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        out["reference"] = {"unavailable": f"ref_gpu exited {r.returncode}: {r.stderr[-300:]}"}
+        return out
+    lines = [json.loads(x) for x in open(res_path)]
+    head, rows = lines[0], lines[1:]
+    ok = [x for x in rows if x["status"] == "ok"]
+    rcounts = [x.get("count") for x in rows]
+    gpu_ms = sum(x["gpu_ms"] for x in ok)
+    ker_ms = sum(x["kernel_ms"] for x in ok)
+    out["reference"] = {
+        "queries_finished": len(ok), "statuses": sorted({x["status"] for x in rows}),
+        "queries_per_s": len(ok) / (gpu_ms / 1000.0) if gpu_ms else None,
+        "gpu_ms_per_query_mean": gpu_ms / len(ok) if ok else None,
+        "kernel_ms_per_query_mean": ker_ms / len(ok) if ok else None,
+        "exact_vs_oracle": all(c == w for c, w in zip(rcounts, want) if c is not None),
+        "data_parse_s": head["parse_s"],
+        "what": "reference kernels hnInit/hnGen/hnCheck/hnRemove compiled for sm_100a, level driver on the "
+                "host (its CDP1 device driver does not build for sm_100a); gpu_ms = planning + table copies + "
+                "level loop + count read, data graph resident",
+    }
+    if ok and len(ok) == len(rows):
+        out["ours_plain_over_reference"] = out["ours_plain"]["queries_per_s"] / out["reference"]["queries_per_s"]
+        out["ours_batched_over_reference"] = (out["ours_batched"]["queries_per_s"] /
+                                              out["reference"]["queries_per_s"])
+    for f in qpaths + [dpath, res_path]:
+        os.unlink(f)
+    os.rmdir(tmp)
+    return out
+
+
+def configs_leg(local, peak_gbs, cap=2_000_000_000):
+    """Configurations 2 and 4 at their stated sizes, beside the headline.
+
+    Config 2 (R-MAT 2^20, 16M undirected edges, unlabelled): the triangle,
+    exact against 6 x the oracle's triangle count, with its own roofline;
+    the 4-cycle, 4-clique and house run under a candidate cap and are
+    reported as capped (their counts need 10^11+ candidates).  Config 4
+    (labelled R-MAT 2^22, average degree 16, 4,096 random-walk queries of
+    3-12 vertices, vertex labels matched): its 3-vertex queries batched and
+    one at a time, every count exact against the fixture
+    (tests/golden/config_counts.json); a sample of its larger queries under
+    the cap, reported as capped.  Each capped query is a GFSM_ERR_TOO_LARGE
+    return, never a count."""
+    import gfsm_b200
+    from gfsm_b200 import synth
+    try:
+        gold = json.load(open(os.path.join(ROOT, "tests", "golden", "config_counts.json")))
+    except Exception:
+        return {"unavailable": "tests/golden/config_counts.json missing"}
+    out = {"candidate_cap": cap}
+    # -- config 2
+    t0 = time.perf_counter()
+    g2, shapes = synth.config2()
+    ctx2 = gfsm_b200.GFSM(device=local)
+    s, d = g2.directed()
+    n2 = g2.n
+    data2 = ctx2.graph_from_edges(n2, s, d).to_device()
+    del g2
+    names = ("triangle", "4-cycle", "4-clique", "house")
+    plans2 = [ctx2.pre_process_query(ctx2.graph_from_edges(q.n, *q.directed())) for q in shapes]
+    ctx2.match_count(plans2[0], data2)
+    ms, stt = [], None
+    for _ in range(3):
+        c, stt = ctx2.match_count(plans2[0], data2)
+        ms.append(stt["device_ms"])
+    tri_ms = float(np.median(ms))
+    c2 = {"triangle": {"count": c, "exact": c == gold["config2"]["triangle"], "device_ms": tri_ms,
+                       "candidates": stt["candidates"], "embeddings_per_s": c / (tri_ms / 1000.0),
+                       "roofline": {"bound": "hbm", "achieved": stt["alg_bytes"] / (tri_ms / 1000.0) / 1e9,
+                                    "peak": peak_gbs, "unit": "GB/s",
+                                    "frac": stt["alg_bytes"] / (tri_ms / 1000.0) / 1e9 / peak_gbs}}}
+    ctx2.close()
+    ctx2c = gfsm_b200.GFSM(device=local, max_candidates=cap)
+    data2c = ctx2c.graph_from_edges(n2, s, d).to_device()
+    del s, d
+    for name, q in zip(names[1:], shapes[1:]):
+        plan = ctx2c.pre_process_query(ctx2c.graph_from_edges(q.n, *q.directed()))
+        try:
+            c, st = ctx2c.match_count(plan, data2c)
+            c2[name] = {"count": c, "exact": None, "device_ms": st["device_ms"]}
+        except gfsm_b200.GFSMError as e:
+            c2[name] = {"capped": True, "status": e.status}
+    ctx2c.close()
+    c2["seconds"] = time.perf_counter() - t0
+    out["config2"] = c2
+    # -- config 4
+    t0 = time.perf_counter()
+    g4, qs = synth.config4(nq=4096)
+    want = dict(zip(gold["config4"]["indices"], gold["config4"]["counts"]))
+    ctx4 = gfsm_b200.GFSM(device=local, vertex_labels=1)
+    s, d = g4.directed()
+    data4 = ctx4.graph_from_edges(g4.n, s, d, None, g4.vlabel).to_device()
+    idx = sorted(want)
+    sub = [qs[i] for i in idx]
+    plans4 = ctx4.prepare_queries([(q.n,) + tuple(q.directed()) + (None, q.vlabel) for q in sub])
+    ctx4.batch_count(plans4, data4)
+    bc, bst = ctx4.batch_count(plans4, data4)
+    lat, pc = [], []
+    for p in plans4:
+        t1 = time.perf_counter()
+        c, _ = ctx4.match_count(p, data4)
+        lat.append(time.perf_counter() - t1)
+        pc.append(c)
+    exact4 = bc.tolist() == [want[i] for i in idx] and pc == bc.tolist()
+    c4 = {"three_vertex": {"queries": len(idx), "exact": exact4,
+                           "batched_queries_per_s": len(idx) / (bst["device_ms"] / 1000.0),
+                           "plain_queries_per_s": len(idx) / sum(lat), "batch_device_ms": bst["device_ms"],
+                           "embeddings": int(bc.sum())}}
+    ctx4.close()
+    ctx4c = gfsm_b200.GFSM(device=local, vertex_labels=1, max_candidates=cap)
+    data4c = ctx4c.graph_from_edges(g4.n, s, d, None, g4.vlabel).to_device()
+    larger = [q for q in qs if q.n > 3][:16]
+    capped = finished = 0
+    for q in larger:
+        plan = ctx4c.pre_process_query(ctx4c.graph_from_edges(q.n, *q.directed(), None, q.vlabel))
+        try:
+            ctx4c.match_count(plan, data4c)
+            finished += 1
+        except gfsm_b200.GFSMError:
+            capped += 1
+    ctx4c.close()
+    c4["larger_sample"] = {"queries": len(larger), "finished_under_cap": finished, "capped": capped}
+    c4["seconds"] = time.perf_counter() - t0
+    out["config4"] = c4
+    out["exact"] = bool(c2["triangle"]["exact"] and exact4)
+    return out
+
+
 def run_reference(args, rank, world, pg):
     if rank != 0:
         return
@@ -321,6 +512,7 @@ def run_ours(args, rank, world, local, pg):
     # -- device-resident batched steps
     clocks = Clocks(local)
     dev_ms, k_ms, alg, launches, step_launches, cand, expans, embeds = [], 0.0, 0, 0, 0, 0, 0, 0
+    drivers = set()
     barrier(pg)
     torch.cuda.synchronize(local)
     clocks.start()
@@ -332,6 +524,7 @@ def run_ours(args, rank, world, local, pg):
         k_ms += st["kernel_ms"]
         alg += st["alg_bytes"]
         launches += st["launches"]          # every kernel of the call
+        drivers.add((st["tile_variant"], st["driver"], st["graph_error"]))
         step_launches += st["steps"]        # level-step kernels
         expans += st["expansions"]
         embeds += int(counts.sum())
@@ -443,6 +636,16 @@ def run_ours(args, rank, world, local, pg):
             "alg_bytes_per_step": alg / args.steps, "kernel_ms_per_step": k_ms / args.steps,
             "candidates_per_s": cand / (k_ms / 1000.0) if k_ms else 0.0}
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = configs_leg(local, pk["hbm_gbs"])
+        exact = exact and configs.get("exact", True)
+
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = ref_gpu_leg(g, qs, local)
+        exact = exact and all(v.get("exact_vs_oracle", True) for v in ref_gpu.values() if isinstance(v, dict))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         co = CpuOracle(g)
@@ -472,7 +675,10 @@ def run_ours(args, rank, world, local, pg):
             "plain": plain, "served": served, "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
-            "clocks": clk, "gpu_launches": launches, "ingest": ingest, "planner": planner,
+            "schedule": [{"tile_variant": v, "driver": "graph" if dr else "host loop", "graph_error": ge}
+                         for v, dr, ge in sorted(drivers)],
+            "clocks": clk, "gpu_launches": launches, "ingest": ingest, "planner": planner, "ref_gpu": ref_gpu,
+            "configs": configs,
             "work": {"partial_mappings_per_s": expans / (sum(dev_ms) / 1000.0),
                      "embeddings_per_s": embeds / (sum(dev_ms) / 1000.0),
                      "candidates_per_s": cand / (sum(dev_ms) / 1000.0),
