@@ -380,6 +380,12 @@ class GFSM:
                                                   b.ctypes.data_as(_lib.u64p)))
         return lo.value, b
 
+    def predict_frontier_bytes(self, plan, data):
+        """The served form's admission estimate of plan's peak frontier bytes."""
+        b = C.c_double()
+        self._check(self._lib.gfsm_predict_frontier_bytes(self._h, plan.handle, data.handle, C.byref(b)))
+        return b.value
+
     def serve(self, data, **kw):
         return Server(self, data, **kw)
 

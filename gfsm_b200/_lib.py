@@ -46,6 +46,7 @@ SIGNATURES = {
     "gfsm_partition_rows": (C.c_int, [u32p, C.c_uint32, C.c_uint32, C.c_uint32, u64p]),
     "gfsm_root_partition": (C.c_int, [vp, vp, vp, C.c_uint32, u32p, u64p]),
     "gfsm_batch_count_part": (C.c_int, [vp, C.POINTER(vp), C.c_int, vp, C.c_uint32, C.c_uint32, u64p, vp]),
+    "gfsm_predict_frontier_bytes": (C.c_int, [vp, vp, vp, C.POINTER(C.c_double)]),
     "gfsm_serve_start": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "gfsm_serve_submit": (C.c_int, [vp, vp, C.c_uint64]),
     "gfsm_serve_poll": (C.c_int, [vp, vp, C.c_int, C.POINTER(C.c_int)]),

@@ -153,17 +153,32 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
     BCHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (cudaEvent_t &e : ev) BCHECK(cudaEventCreate(&e));
     if (vl_mode) {
-        std::vector<uint32_t> vals(h.vlabel.begin(), h.vlabel.end());
-        std::sort(vals.begin(), vals.end());
-        vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
-        out.group_value = vals;
+        // label value -> group (labels ascending): a table over the value
+        // range when it is small (the usual case), else a sort of the values
+        uint32_t mx = 0;
+        for (uint32_t v = 0; v < n; ++v) mx = std::max(mx, h.vlabel[v]);
+        std::vector<uint32_t> vals;
         group.resize(n);
-        std::vector<uint32_t> cnt(vals.size() + 1, 0);
-        for (uint32_t v = 0; v < n; ++v) {
-            group[v] = (uint32_t)(std::lower_bound(vals.begin(), vals.end(), h.vlabel[v]) - vals.begin());
-            cnt[group[v] + 1]++;
+        if (mx < (1u << 22)) {
+            std::vector<uint32_t> idx((size_t)mx + 1, 0);
+            for (uint32_t v = 0; v < n; ++v) idx[h.vlabel[v]] = 1;
+            for (uint32_t x = 0; x <= mx; ++x)
+                if (idx[x]) {
+                    idx[x] = (uint32_t)vals.size();
+                    vals.push_back(x);
+                }
+            for (uint32_t v = 0; v < n; ++v) group[v] = idx[h.vlabel[v]];
+        } else {
+            vals.assign(h.vlabel.begin(), h.vlabel.end());
+            std::sort(vals.begin(), vals.end());
+            vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+            for (uint32_t v = 0; v < n; ++v)
+                group[v] = (uint32_t)(std::lower_bound(vals.begin(), vals.end(), h.vlabel[v]) - vals.begin());
         }
+        std::vector<uint32_t> cnt(vals.size() + 1, 0);
+        for (uint32_t v = 0; v < n; ++v) cnt[group[v] + 1]++;
         for (size_t i = 0; i < vals.size(); ++i) cnt[i + 1] += cnt[i];
+        out.group_value = vals;
         out.group_start = cnt;
     } else {
         out.group_value = {0};

@@ -135,7 +135,6 @@ struct StepArgs {
     uint64_t cstride, ccap;
     uint32_t *ccstart;
     unsigned long long *ccoff;                      // [ccap+1]
-    uint32_t *tile_ctr;                             // tile queue of the fixed-grid step kernel
     // results
     unsigned long long *counts;                     // per query
     StepResult *result;
@@ -161,12 +160,11 @@ constexpr uint32_t kBranch = 1u << 31;
 // no tile of that step had to wait for the others to publish it.
 __global__ void k_partition(unsigned long long *coff, uint64_t np, unsigned long long coff_end,
                             unsigned long long c0, unsigned long long ncand, uint32_t ntiles, uint32_t tile_size,
-                            uint32_t *__restrict__ tile_parent, uint32_t *tile_ctr, StepResult *result,
+                            uint32_t *__restrict__ tile_parent, StepResult *result,
                             unsigned long long *step_counts, uint32_t nq) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     for (uint32_t i = t; i < nq; i += gridDim.x * blockDim.x) step_counts[i] = 0;
     if (t == 0) {
-        *tile_ctr = 0;
         *result = StepResult{};
         coff[np] = coff_end;  // the searches below read coff[0, np) only
     }
@@ -635,13 +633,11 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         if (sm.fcount) atomicAdd(&a.counts[sm.q0], sm.fcount);
     }
     __syncthreads();
-    // ---- write the tile's children: consecutive threads -> consecutive slots
-    const unsigned long long ex_cnt = sm.excl_cnt, ex_deg = sm.excl_deg;
-    const uint32_t ntot = sm.wofs[NWARP];
-    for (uint32_t i = tid; i < ntot; i += T) {
-        uint32_t w = 0;
-        while (w + 1 < (uint32_t)NWARP && sm.wofs[w + 1] <= i) ++w;
-        const Stage r = sm.stage[w * WC + (i - sm.wofs[w])];
+    // ---- write the tile's children: every warp writes its own packed
+    // survivors to its consecutive range of the tile's slots
+    const unsigned long long ex_cnt = sm.excl_cnt + sm.wofs[warp], ex_deg = sm.excl_deg + sm.wdofs[warp];
+    for (uint32_t i = lane; i < wcnt; i += 32) {
+        const Stage r = wstage[i];
         const uint64_t slot = ex_cnt + i;
         if (slot >= a.ccap) continue;  // overflow: the host retries with a smaller chunk
         a.ctup[slot] = r.q;
@@ -649,7 +645,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             a.ctup[(uint64_t)(1 + k) * a.cstride + slot] = __ldg(a.ptup + (uint64_t)(1 + k) * a.pstride + r.p);
         a.ctup[(uint64_t)(1 + d) * a.cstride + slot] = r.v;
         a.ccstart[slot] = r.cs;
-        a.ccoff[slot] = ex_deg + sm.wdofs[w] + r.cnt;
+        a.ccoff[slot] = ex_deg + r.cnt;
     }
 }
 
@@ -706,6 +702,7 @@ struct Ctl {
     uint32_t tile;                     // candidates per tile of the graph's step kernel
     unsigned long long chunk, max_scan, max_candidates;
     unsigned long long steps, retries, candidates, expansions, alg_bytes;
+    unsigned long long held[MAXQ], peak;  // tuples each depth's buffer holds; largest bytes held at once
     uint32_t d, dmax, emits, done, err;
 };
 
@@ -762,7 +759,6 @@ __device__ void ctl_plan(Ctl &c) {
     }
     c.chunk = chunk;
     c.emits = emits;
-    *a.tile_ctr = 0;
     *a.result = StepResult{};
 }
 
@@ -799,6 +795,10 @@ __device__ void ctl_after(Ctl &c) {
     }
     c.pos[d] += c.chunk;
     if (c.emits) {
+        c.held[d] = n;
+        unsigned long long live = 0;  // the buffers of depths <= d are live now
+        for (uint32_t i = 0; i <= d; ++i) live += c.held[i] * tuple_bytes(i);
+        if (live > c.peak) c.peak = live;
         c.ratio[d] = (float)fmax(2.0 * (double)n / (double)c.chunk, (double)c.ratio[d] * 0.5);
         if (n > 0 && next > 0) {
             c.np[d + 1] = n;
@@ -859,25 +859,22 @@ __global__ void k_part_g(const Ctl *ctl) {
     }
 }
 
-// Graph node: the level step on a fixed grid; every CTA takes tiles from the
-// step's tile queue.  One instantiation per argument slot and tile geometry.
-template <int SLOT, class G>
+// Graph nodes: the level step on a fixed grid; every CTA takes tiles from
+// the step's tile queue.  One instantiation per argument slot, tile geometry
+// and step kind: the root step and the deeper levels are separate nodes, and
+// the one whose kind the step is not returns at once (one kernel holding both
+// had twice the code and spilled).
+template <int SLOT, class G, bool ROOT>
 __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
     __shared__ StepSmem<G> sm;
-    __shared__ uint32_t s_tile[2];
     const StepArgs &a = c_args[SLOT];
-    // the next tile is fetched while this one runs (double-buffered: a slot
-    // is rewritten only after every thread has passed the barrier that
-    // follows its read)
-    if (threadIdx.x == 0) s_tile[0] = atomicAdd(a.tile_ctr, 1u);
-    __syncthreads();
-    uint32_t tile = s_tile[0];
-    for (uint32_t it = 1; tile < a.ntiles; ++it) {
-        if (threadIdx.x == 0) s_tile[it & 1u] = atomicAdd(a.tile_ctr, 1u);
-        if (a.depth == 0) step_tile<true, G>(a, tile, sm);
-        else step_tile<false, G>(a, tile, sm);
+    if ((a.depth == 0) != ROOT) return;
+    // tiles are dealt out grid-stride: a shared tile counter taken with an
+    // atomic per tile stalled every tile's start on an address all resident
+    // CTAs contend for (grid batch 132 ms against 115 ms of separate launches)
+    for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        step_tile<ROOT, G>(a, tile, sm);
         __syncthreads();
-        tile = s_tile[it & 1u];
     }
 }
 
@@ -887,13 +884,17 @@ __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
 constexpr int kGraphGeos = 2;
 constexpr int graph_geo(int variant) { return variant == 0 ? 0 : variant == 2 ? 1 : -1; }
 
+// Graph node kernels of argument slot s and graph geometry ggeo: kind 0 the
+// tile directory, 1 the root step, 2 the deeper levels' step.
 template <int... S>
-const void *slot_kernel(int s, int ggeo, bool step) {
+const void *slot_kernel(int s, int ggeo, int kind) {
     static const void *part[kGraphGeos][sizeof...(S)] = {{(const void *)k_part_g<S, Geo0::TILE>...},
                                                           {(const void *)k_part_g<S, Geo2::TILE>...}};
-    static const void *stepk[kGraphGeos][sizeof...(S)] = {{(const void *)k_step_g<S, Geo0>...},
-                                                           {(const void *)k_step_g<S, Geo2>...}};
-    return step ? stepk[ggeo][s] : part[ggeo][s];
+    static const void *root[kGraphGeos][sizeof...(S)] = {{(const void *)k_step_g<S, Geo0, true>...},
+                                                          {(const void *)k_step_g<S, Geo2, true>...}};
+    static const void *stepk[kGraphGeos][sizeof...(S)] = {{(const void *)k_step_g<S, Geo0, false>...},
+                                                           {(const void *)k_step_g<S, Geo2, false>...}};
+    return kind == 0 ? part[ggeo][s] : kind == 1 ? root[ggeo][s] : stepk[ggeo][s];
 }
 
 inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
@@ -1087,16 +1088,14 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     ECHECK(cudaMallocHost(&h_result, sizeof(StepResult)));
     max_scan = std::min<uint64_t>(std::max<uint64_t>(scan_limit, TILE), 1ull << 31);
     dir_tiles = (uint32_t)div_up(max_scan, kMinTile);
-    // small region: result, counters, tile directory, schedule control block
+    // small region: result, mapping-row counter, tile directory, schedule control block
     small_bytes = 512 + ((((uint64_t)dir_tiles + 2) * 4 + 255) & ~255ull) + ((sizeof(Ctl) + 255) & ~255ull);
     ECHECK(cudaMalloc(&small, small_bytes));
     ECHECK(cudaMemsetAsync(small, 0, small_bytes, stream));
     char *p = static_cast<char *>(small);
     static_assert(sizeof(StepResult) <= 64, "StepResult fits its slot");
     d_result = reinterpret_cast<StepResult *>(p);
-    p += 64;
-    tile_ctr = reinterpret_cast<uint32_t *>(p);
-    p += 64;
+    p += 128;
     rows_ctr = reinterpret_cast<uint32_t *>(p);
     p += 64;
     tile_parent = reinterpret_cast<uint32_t *>(p);
@@ -1106,8 +1105,8 @@ gfsm_status Engine::init(int dev, uint64_t arena_limit, uint64_t scan_limit, std
     {
         int sms = 0, per_sm0 = 0, per_sm2 = 0;
         ECHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, k_step_g<0, Geo0>, Geo0::T, 0));
-        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_step_g<0, Geo2>, Geo2::T, 0));
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm0, k_step_g<0, Geo0, false>, Geo0::T, 0));
+        ECHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_step_g<0, Geo2, false>, Geo2::T, 0));
         step_blocks[graph_geo(0)] = sms * std::max(per_sm0, 1);
         step_blocks[graph_geo(2)] = sms * std::max(per_sm2, 1);
     }
@@ -1177,15 +1176,18 @@ gfsm_status Engine::build_graph(int variant, std::string &err) {
     if ((e = cudaGraphAddMemcpyNodeToSymbol(&b0, body, nullptr, 0, c_args, &cp->args, sizeof(StepArgs),
                                             (size_t)slot * sizeof(StepArgs), cudaMemcpyDeviceToDevice)) != cudaSuccess)
         return fail(e, "args copy node");
-    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, false));
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, 0));
     kp.gridDim = dim3((unsigned)step_blocks[gg]);
     kp.blockDim = dim3(256);
     kp.kernelParams = a_part;
     if ((e = cudaGraphAddKernelNode(&b1, body, &b0, 1, &kp)) != cudaSuccess) return fail(e, "partition node");
-    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, true));
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, 1));
     kp.blockDim = dim3(gg == 0 ? Geo0::T : Geo2::T);
     kp.kernelParams = nullptr;
-    if ((e = cudaGraphAddKernelNode(&b2, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "step node");
+    cudaGraphNode_t b1r;
+    if ((e = cudaGraphAddKernelNode(&b1r, body, &b1, 1, &kp)) != cudaSuccess) return fail(e, "root step node");
+    kp.func = const_cast<void *>(slot_kernel<0, 1, 2, 3, 4, 5, 6, 7>(slot, gg, 2));
+    if ((e = cudaGraphAddKernelNode(&b2, body, &b1r, 1, &kp)) != cudaSuccess) return fail(e, "step node");
     kp.func = (void *)k_ctl;
     kp.gridDim = dim3(1);
     kp.blockDim = dim3(256);
@@ -1522,7 +1524,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         // every depth buffer starts on a 256-byte boundary (u64 coff arrays)
         const uint64_t share = dmax ? (rest / dmax) & ~255ull : 0;
         for (uint32_t d = 0; d < dmax; ++d) {
-            const uint64_t per = 4ull * (d + 2) + 4 + 8;
+            const uint64_t per = tuple_bytes(d);
             uint64_t cap = share > 1024 ? (share - 1024) / per : 0;
             cap = std::min<uint64_t>(cap, lim.max_soln_size);
             cap = std::min<uint64_t>(cap, 0xffffffffull);
@@ -1541,7 +1543,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
                 return GFSM_ERR_CUDA;
             }
         }
-        st.peak_frontier_bytes = budget;
     }
 
     GraphView gv{g.rowptr, g.adj, g.elab, g.order, g.single_label, g.n};
@@ -1586,7 +1587,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.g = gv;
         a.plans = d_plans;
         a.tile_parent = tile_parent;
-        a.tile_ctr = tile_ctr;
         a.counts = d_step_counts;
         a.result = d_result;
         a.rows_out = d_rows;
@@ -1609,7 +1609,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         st.steps = c.steps;
-        st.launches = (uint32_t)(1 + 3 * c.steps);  // first controller, then partition, step, controller per step
+        st.peak_frontier_bytes = c.peak;
+        st.launches = (uint32_t)(1 + 4 * c.steps);  // first controller, then partition, root step, step, controller
         st.retries = c.retries;
         st.candidates = c.candidates;
         st.expansions = c.expansions;
@@ -1638,7 +1639,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (stats) *stats = st;
         return GFSM_OK;
     }
-    std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0);
+    std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0), held(dmax + 1, 0);
     std::vector<double> ratio(dmax + 1, ratio_init);
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) has_final[q.k - 1] = 1;
@@ -1689,7 +1690,6 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             a.ccstart = buf[d].cstart;
             a.ccoff = buf[d].coff;
         }
-        a.tile_ctr = tile_ctr;
         a.counts = d_step_counts;
         a.result = d_result;
         a.rows_out = d_rows;
@@ -1699,8 +1699,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.fan_list = d_fan_list;
         a.pcoff_end = total[d];
         k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, ne), 256), 256, 0, stream>>>(
-            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, vtile, tile_parent, tile_ctr, d_result, d_step_counts,
-            ne);
+            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, vtile, tile_parent, d_result, d_step_counts, ne);
         ECHECK(cudaEventRecord(ev0, stream));
         launch_step(variant, d == 0, a, ntiles, stream);
         ECHECK(cudaGetLastError());
@@ -1748,6 +1747,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         st.alg_bytes += r.alg_bytes + (emits ? r.n_children * 4ull * (d + 1) : 0ull);
         pos[d] += chunk;
         if (emits) {
+            held[d] = r.n_children;
+            unsigned long long live = 0;  // the buffers of depths <= d are live now
+            for (uint32_t i = 0; i <= d; ++i) live += held[i] * tuple_bytes(i);
+            st.peak_frontier_bytes = std::max<uint64_t>(st.peak_frontier_bytes, live);
             const double obs = (double)r.n_children / (double)chunk;
             ratio[d] = std::max(2.0 * obs, ratio[d] * 0.5);
             if (r.n_children > 0 && r.total_next > 0) {
@@ -1872,8 +1875,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
     unsigned char *p = scratch;
     StepResult *d_result = reinterpret_cast<StepResult *>(p);
     p += 256;
-    uint32_t *tile_ctr = reinterpret_cast<uint32_t *>(p);
-    uint32_t *rows_ctr = tile_ctr + 16;
+    uint32_t *rows_ctr = reinterpret_cast<uint32_t *>(p);
     p += 256;
     uint32_t *tile_parent = reinterpret_cast<uint32_t *>(p);
     p += (((uint64_t)kNoAllocTiles + 2) * 4 + 255) & ~255ull;
@@ -1964,7 +1966,6 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
             a.ccstart = buf[d].cstart;
             a.ccoff = buf[d].coff;
         }
-        a.tile_ctr = tile_ctr;
         a.counts = d_count;
         a.result = d_result;
         a.rows_ctr = rows_ctr;
@@ -1973,7 +1974,7 @@ extern "C" gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfs
         // step never counts twice and the count goes straight to the total
         a.pcoff_end = total[d];
         k_partition<<<(unsigned)div_up((uint64_t)ntiles + 1, 256), 256, 0, st>>>(
-            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, TILE, tile_parent, tile_ctr, d_result, nullptr, 0);
+            a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, TILE, tile_parent, d_result, nullptr, 0);
         launch_step(0, d == 0, a, ntiles, st);
         if (cudaGetLastError() != cudaSuccess) return fail(GFSM_ERR_CUDA);
         StepResult r;

@@ -24,7 +24,6 @@ struct Engine {
     StepResult *h_result = nullptr;  // pinned
     void *h_stage = nullptr;         // pinned staging of a call's arena head (plans, root tables, ...)
     uint64_t h_stage_bytes = 0;
-    uint32_t *tile_ctr = nullptr;
     uint32_t *rows_ctr = nullptr;
     uint32_t *tile_parent = nullptr;
     uint64_t max_scan = 0;

@@ -173,6 +173,7 @@ struct gfsm_graph {
     bool vl_mode = false;
     std::mutex stats_mu;
     std::unique_ptr<gfsm::PlanStats> stats;
+    std::vector<double> deg2;  // prefix sums of squared row lengths (served form's predictor)
 };
 
 struct gfsm_plan {
@@ -200,6 +201,12 @@ void free_device_graph(DeviceGraph &g);
 // multiplies the count by p.aut).
 gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim,
                          DQuery &dq, uint32_t &root_lo, uint32_t &root_hi, bool &never, bool sym = false);
+// Device bytes one partial mapping of depth d's buffer takes: query id and
+// d+1 tuple columns, its next-level slice start and candidate prefix.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr unsigned long long tuple_bytes(uint32_t d) { return 4ull * (d + 2) + 4 + 8; }
 // Degree-balanced cut of a root window [lo, hi) of internal ids into nparts
 // consecutive ranges: bounds[0..nparts] are offsets into the window, part k
 // is [lo + bounds[k], lo + bounds[k+1]), and each part's rows hold about

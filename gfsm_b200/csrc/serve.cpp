@@ -33,27 +33,65 @@ struct Req {
     double pred_bytes;
 };
 
-// Predicted peak frontier bytes of one query: roots times the average
-// candidate slice per level, each level's tuples kept until the next one.
-double predict_bytes(const Plan &p, const DeviceGraph &g, const gfsm_limits &lim) {
+}  // namespace
+
+namespace gfsm {
+
+// Prefix sums of squared row lengths over internal ids (deg2[i] = sum of
+// deg(v)^2 for v < i), built once per data graph on first use.
+const std::vector<double> &graph_deg2(const gfsm_graph *data) {
+    gfsm_graph *g = const_cast<gfsm_graph *>(data);
+    std::lock_guard<std::mutex> lk(g->stats_mu);
+    if (g->deg2.empty()) {
+        const DeviceGraph &d = *data->dev;
+        g->deg2.resize((size_t)d.n + 1);
+        g->deg2[0] = 0.0;
+        for (uint32_t v = 0; v < d.n; ++v) {
+            const double x = (double)(d.h_rowptr[v + 1] - d.h_rowptr[v]);
+            g->deg2[v + 1] = g->deg2[v] + x * x;
+        }
+    }
+    return g->deg2;
+}
+
+// Predicted peak frontier bytes of one query: the partial mappings of every
+// non-final depth held at once, each level's count the previous one's times
+// its expected candidate slice times 1/2 per extra requirement.  The
+// expected slice of a parent is the anchor's expected row length -- the
+// size-biased mean deg^2 / deg over the anchor's window, since the anchor
+// was itself reached along an edge (the plain mean for the root) -- times
+// the share of all CCSR entries that land in the new vertex's window.
+double predict_bytes(const Plan &p, const DeviceGraph &g, const std::vector<double> &deg2, const gfsm_limits &lim) {
     DQuery dq;
     uint32_t lo = 0, hi = 0;
     bool never = false;
-    if (build_dquery(p, g, lim, dq, lo, hi, never) != GFSM_OK || never) return 0.0;
-    const double avg_deg = g.n ? (double)g.m / (double)g.n : 0.0;
-    double frontier = (double)(hi - lo), peak = 0.0;
+    if (build_dquery(p, g, lim, dq, lo, hi, never) != GFSM_OK || never || g.m == 0) return 0.0;
+    const double vol_all = (double)g.m;
+    auto vol = [&](uint32_t a, uint32_t b) { return (double)(g.h_rowptr[b] - g.h_rowptr[a]); };
+    std::vector<double> f(p.k, 0.0);
+    f[0] = (double)(hi - lo);
+    double peak = 0.0, live = 0.0;
     for (uint32_t d = 1; d < p.k; ++d) {
         const DLevel &L = dq.lv[d];
-        const double window = g.n ? (double)(L.hi - L.lo) / (double)g.n : 0.0;
-        const double sel = d >= 2 ? 0.5 : 1.0;  // each extra requirement prunes
-        frontier *= std::max(1.0, avg_deg * window * sel);
-        if (d + 1 < p.k) peak = std::max(peak, frontier * (4.0 * (d + 2) + 12.0));
+        const uint32_t a = L.anchor;  // tuple position of the anchor
+        const DLevel &A = dq.lv[a];
+        const double va = vol(A.lo, A.hi);
+        const double row = va <= 0.0 ? 0.0
+                           : a == 0 ? va / std::max(1.0, (double)(A.hi - A.lo))
+                                    : (deg2[A.hi] - deg2[A.lo]) / va;
+        double grow = row * vol(L.lo, L.hi) / vol_all;
+        for (uint32_t r = 0; r < L.nreq; ++r) grow *= 0.5;
+        f[d] = f[d - 1] * grow;
+        if (d + 1 < p.k) {
+            live += f[d] * (double)tuple_bytes(d);
+            peak = std::max(peak, live);
+        }
         if (peak > 1e18) break;
     }
     return peak;
 }
 
-}  // namespace
+}  // namespace gfsm
 
 struct gfsm_server {
     gfsm_ctx *ctx = nullptr;
@@ -172,12 +210,21 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
     return GFSM_OK;
 }
 
+gfsm_status gfsm_predict_frontier_bytes(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data,
+                                        double *bytes) {
+    if (!ctx || !plan || !data || !bytes) return GFSM_ERR_ARG;
+    gfsm_status rc = gfsm_graph_to_device(ctx, const_cast<gfsm_graph *>(data));
+    if (rc != GFSM_OK) return rc;
+    *bytes = predict_bytes(plan->p, *data->dev, graph_deg2(data), ctx->lim);
+    return GFSM_OK;
+}
+
 gfsm_status gfsm_serve_submit(gfsm_server *s, const gfsm_plan *plan, uint64_t req_id) {
     if (!s || !plan) return GFSM_ERR_ARG;
     Req r;
     r.id = req_id;
     r.plan = plan->p;
-    r.pred_bytes = predict_bytes(r.plan, *s->data->dev, s->ctx->lim);
+    r.pred_bytes = predict_bytes(r.plan, *s->data->dev, graph_deg2(s->data), s->ctx->lim);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) return GFSM_ERR_STOPPED;

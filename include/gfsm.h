@@ -85,7 +85,8 @@ typedef struct {
     uint64_t alg_bytes;          /* algorithmic bytes (parent tuples + backward-neighbour rows + child tuples) */
     uint64_t steps;              /* frontier steps launched                        */
     uint64_t retries;            /* steps re-run with a smaller chunk              */
-    uint64_t peak_frontier_bytes;/* device bytes of the frontier arena in use     */
+    uint64_t peak_frontier_bytes;/* most device bytes of partial mappings held at once
+                                    (measured: the live depth buffers after each step) */
     double   kernel_ms;          /* device time of the level-step kernels (sum)    */
     double   device_ms;          /* device timeline of the call: first step to last */
     double   wall_ms;            /* host wall time of the call                     */
@@ -263,6 +264,12 @@ gfsm_status gfsm_batch_count_part(gfsm_ctx *ctx, const gfsm_plan *const *plans, 
 /* --- serving ------------------------------------------------------------ */
 gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_serve_config *cfg,
                              gfsm_server **out);
+/* The served form's admission estimate of a query's peak frontier bytes on
+ * `data` (no counterpart in the reference): level counts grown by each
+ * level's expected candidate slice and halved per extra requirement; the
+ * measured peak of a call is gfsm_stats.peak_frontier_bytes. */
+gfsm_status gfsm_predict_frontier_bytes(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm_graph *data,
+                                        double *bytes);
 /* The plan is copied; the caller may destroy it after the call. */
 gfsm_status gfsm_serve_submit(gfsm_server *s, const gfsm_plan *plan, uint64_t req_id);
 /* Non-blocking; returns up to max finished results. */
