@@ -208,8 +208,11 @@ def traffic_record():
 
 
 class CpuOracle:
-    """The oracle's restatement of the reference's FFS algorithm on the host
-    cores (all threads), over the same data graph and queries."""
+    """The oracle on the host cores (all threads unless told otherwise), over
+    the same data graph and queries: `ffs` = its restatement of the
+    reference's FFS algorithm (the reference arm), `bt` = the independent
+    backtracking enumerator (the CPU baseline).  Query parsing and planning
+    happen before the timed loop; only the counting is timed."""
 
     def __init__(self, g, threads=None):
         import tempfile
@@ -221,17 +224,36 @@ class CpuOracle:
         dpath = os.path.join(self.tmp, "d.g")
         g.write_text(dpath)
         self.od = oracle.Graph(path=dpath)
+        self.g = g
+        self.ds, self.dd = g.directed()
 
-    def run(self, qs, budget_s):
-        """Queries from the front of qs until budget_s is spent."""
+    def prepare(self, qs, kind):
+        o = self.oracle
+        out = []
+        for q in qs:
+            if kind == "ffs":
+                qp = os.path.join(self.tmp, "q.g")
+                q.write_text(qp)
+                oq = o.Graph(path=qp)
+                out.append((oq, o.Plan(oq)))
+            else:
+                qs_, qd_ = q.directed()
+                out.append((q.n, qs_, qd_, q.vlabel))
+        return out
+
+    def run(self, prepared, kind, budget_s):
+        """Queries from the front until budget_s of counting is spent."""
         o = self.oracle
         done, counts = 0, []
         t0 = time.perf_counter()
-        for q in qs:
-            qp = os.path.join(self.tmp, "q.g")
-            q.write_text(qp)
-            oq = o.Graph(path=qp)
-            counts.append(o.ffs_count(oq, o.Plan(oq), self.od, vlabel_mode=True, threads=self.threads))
+        for item in prepared:
+            if kind == "ffs":
+                oq, plan = item
+                counts.append(o.ffs_count(oq, plan, self.od, vlabel_mode=True, threads=self.threads))
+            else:
+                n, qs_, qd_, qvl = item
+                counts.append(o.bt_count(n, qs_, qd_, None, qvl, self.g.n, self.ds, self.dd, None, self.g.vlabel,
+                                         vlabel_mode=True, threads=self.threads))
             done += 1
             if time.perf_counter() - t0 > budget_s:
                 break
@@ -433,10 +455,11 @@ def run_reference(args, rank, world, pg):
     g, qs = make_workload(0, args.queries)
     cpu = CpuOracle(g)
     threads = cpu.threads
+    prepared = cpu.prepare(qs[:2048], "ffs")
     per_step = []
     total_q = 0
     for i in range(args.warmup + args.steps):
-        done, el, _ = cpu.run(qs, budget_s=8.0)
+        done, el, _ = cpu.run(prepared, "ffs", budget_s=8.0)
         if i >= args.warmup:
             per_step.append((done, el))
             total_q += done
@@ -600,7 +623,7 @@ def run_ours(args, rank, world, local, pg):
         rng = np.random.default_rng(5)
         for rate in SERVE_RATES:
             n = min(len(plans), SERVE_REQUESTS)
-            srv = ctx.serve(data, slots=2, max_batch=256)
+            srv = ctx.serve(data, slots=2, max_batch=1024)
             gaps = rng.exponential(1.0 / rate, n)
             gc.collect()
             gc.disable()
@@ -655,14 +678,16 @@ def run_ours(args, rank, world, local, pg):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         co = CpuOracle(g)
-        done, el, ccounts = co.run(qs, budget_s=15.0)
+        prepared = co.prepare(qs[:1024], "bt")
+        done, el, ccounts = co.run(prepared, "bt", budget_s=15.0)
         exact = exact and ccounts == ref_counts[:done].tolist()
         cpu = {"value": done / el, "unit": "queries/s", "cores": co.threads, "kind": "port",
-               "sample": f"first {done} queries of the batch (~15 s of host CPU), oracle restatement of the "
-                         f"reference FFS algorithm"}
+               "sample": f"first {done} queries of the batch (~15 s of host CPU): the oracle's independent "
+                         f"backtracking enumerator, all host threads, query parsing outside the timing; a "
+                         f"reported baseline, not the optimisation target"}
         # the same on one core (a scalar port), over a ~5 s sample
         c1 = CpuOracle(g, threads=1)
-        d1, e1, c1counts = c1.run(qs, budget_s=5.0)
+        d1, e1, c1counts = c1.run(prepared, "bt", budget_s=5.0)
         exact = exact and c1counts == ref_counts[:d1].tolist()
         cpu["single_core"] = {"value": d1 / e1, "unit": "queries/s", "cores": 1, "queries": d1}
 

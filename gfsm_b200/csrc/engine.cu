@@ -882,6 +882,9 @@ __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
 // run the host-driven loop): graph_geo(variant) is the index into them, or
 // -1.
 constexpr int kGraphGeos = 2;
+// First-level candidates (CCSR entries of the root windows) up to which a
+// call runs on the graph by default.
+constexpr uint64_t kGraphRootEntries = 1ull << 22;
 constexpr int graph_geo(int variant) { return variant == 0 ? 0 : variant == 2 ? 1 : -1; }
 
 // Graph node kernels of argument slot s and graph geometry ggeo: kind 0 the
@@ -1265,13 +1268,16 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         const char *t = getenv("GFSM_TRACE");
         return t && *t && *t != '0';
     }();
-    // Driver: GFSM_DRIVER=graph|host forces one.  By default the whole
-    // schedule runs as one CUDA graph launch (no host round trip per step:
-    // plain p50 0.41 -> 0.33 ms on the grid workload) wherever the tile
-    // geometry has a graph; a single query takes the default geometry, a
-    // batch the autotuned one.
+    // Driver: GFSM_DRIVER=graph|host forces one.  By default a light call --
+    // first level of at most kGraphRootEntries candidates over all its
+    // queries -- runs its whole schedule as one CUDA graph launch (no host
+    // round trip per step: plain p50 0.41 -> 0.33 ms on the grid workload);
+    // heavier calls run the host-driven loop, whose steps launch one CTA per
+    // tile (the graph's fixed persistent grid runs a step 10-20% slower).  A
+    // single query takes the default geometry, a batch the autotuned one.
     const char *drv = getenv("GFSM_DRIVER");
-    const bool want_graph = !trace && (drv && *drv ? !strcmp(drv, "graph") : true);
+    const bool force_graph = !trace && drv && *drv && !strcmp(drv, "graph");
+    const bool force_host = trace || (drv && *drv && strcmp(drv, "graph"));
     if (variant < 0) variant = (plans.size() <= 1) ? 0 : pick_variant(plans, g, lim, err);
     auto t_start = std::chrono::steady_clock::now();
     const int nq = (int)plans.size();
@@ -1557,6 +1563,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }();
     // the graph-driven schedule (falls back to the host loop if the graph
     // cannot be built, e.g. when every constant-memory argument slot is taken)
+    uint64_t first_level = 0;  // CCSR entries of the root windows: the first level's candidates, at most
+    for (uint32_t i = 0; i < na && first_level <= kGraphRootEntries; ++i)
+        first_level += (uint64_t)g.h_rowptr[rhi[i]] - g.h_rowptr[rlo[i]];
+    const bool want_graph = !force_host && (force_graph || first_level <= kGraphRootEntries);
     bool graph_driver = false;
     if (want_graph && graph_geo(variant) >= 0) {
         std::string gerr;

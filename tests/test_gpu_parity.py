@@ -290,6 +290,43 @@ def test_device_and_host_drivers_agree(monkeypatch, tile):
     ctx.close()
 
 
+def test_default_driver_policy(monkeypatch):
+    """Without GFSM_DRIVER a call whose first level (the CCSR entries of its
+    queries' root windows) holds at most 2^22 candidates runs on the graph,
+    a heavier one on the host loop; both count what the other driver counts."""
+    monkeypatch.delenv("GFSM_DRIVER", raising=False)
+    monkeypatch.setenv("GFSM_TILE", "0")
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    g = synth.grid(300, 0.05, 0.02, seed=8)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=9)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel).to_device()
+    rowptr = data.download()[0]
+    plans = []
+    for i in range(96):
+        qg, _ = synth.rw_query(g, 3 + i % 6, tree=i % 2 == 0, seed=300 + i)
+        qs, qd = qg.directed()
+        plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+
+    def first_level(ps):
+        tot = 0
+        for p in ps:
+            lo, bounds = ctx.root_partition(p, data, 1)
+            tot += int(rowptr[lo + int(bounds[-1])]) - int(rowptr[lo])
+        return tot
+
+    light, heavy = plans[:1], plans
+    assert first_level(light) <= 1 << 22 < first_level(heavy)
+    for ps, want in ((light, 1), (heavy, 0)):
+        c, st = ctx.batch_count(ps, data)
+        assert st["driver"] == want
+        monkeypatch.setenv("GFSM_DRIVER", "host" if want else "graph")
+        c2, st2 = ctx.batch_count(ps, data)
+        monkeypatch.delenv("GFSM_DRIVER")
+        assert st2["driver"] == 1 - want and c2.tolist() == c.tolist()
+    ctx.close()
+
+
 @pytest.mark.parametrize("variant", ["0", "1", "2", "3"])
 def test_tile_geometries_agree(monkeypatch, variant):
     """Every tile geometry the autotuner can pick gives the same counts,

@@ -229,3 +229,31 @@ def test_symmetry_group_orders_and_limits(host_ctx):
     d = np.array([1, 2, 0, 0], np.uint32)
     p = host_ctx.pre_process_query(host_ctx.graph_from_edges(3, s, d))
     assert p.info()["order_invariant"] is False and p.symmetry() == (1, [])
+
+
+def test_partition_rows_edges():
+    """gfsm_partition_rows: monotone bounds covering the window, parts of
+    near-equal CCSR entries, empty windows, more parts than rows, rows
+    without entries."""
+    import numpy as np
+    import gfsm_b200
+    deg = np.array([9, 7, 7, 5, 3, 3, 2, 1, 1, 1, 0, 0], np.uint32)
+    rowptr = np.zeros(len(deg) + 1, np.uint32)
+    np.cumsum(deg, out=rowptr[1:])
+    for lo, hi in ((0, 12), (2, 9), (5, 5), (10, 12)):
+        for nparts in (1, 2, 3, 5, 16):
+            b = gfsm_b200.partition_rows(rowptr, lo, hi, nparts).astype(np.int64)
+            assert b[0] == 0 and b[-1] == hi - lo and len(b) == nparts + 1
+            assert np.all(np.diff(b) >= 0)
+            w = int(rowptr[hi]) - int(rowptr[lo])
+            if w:
+                parts = [int(rowptr[lo + b[k + 1]]) - int(rowptr[lo + b[k]]) for k in range(nparts)]
+                assert sum(parts) == w
+                # each part ends at the first row reaching its share
+                for k in range(1, nparts):
+                    target = -(-k * w // nparts)
+                    reach = int(rowptr[lo + b[k]]) - int(rowptr[lo])
+                    assert reach >= target
+                    assert b[k] == b[k - 1] or int(rowptr[lo + b[k] - 1]) - int(rowptr[lo]) < target
+    with pytest.raises(gfsm_b200.GFSMError):
+        gfsm_b200.partition_rows(rowptr, 5, 2, 2)
