@@ -687,9 +687,19 @@ void launch_step(int variant, bool root, const StepArgs &a, uint32_t ntiles, cud
 // ---------------------------------------------------------------------------
 static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
 
+// The most candidates an emitting step may take so that its children's
+// next-level candidates, at nxt per candidate (the largest rate seen at this
+// depth; 0: none seen yet), fill at most half the allocator's field.
+__host__ __device__ inline unsigned long long emit_chunk_cap(const double nxt) {
+    if (nxt <= 0.0) return kFirstEmitChunk;
+    const double lim = (double)(kAllocMask / 2) / nxt;
+    return lim < (double)kMaxEmitChunk ? (unsigned long long)(lim > 1.0 ? lim : 1.0) : kMaxEmitChunk;
+}
+
 struct Ctl {
     unsigned long long total[MAXQ + 1], pos[MAXQ + 1], np[MAXQ + 1];
     float ratio[MAXQ + 1];
+    float nxt[MAXQ + 1];         // next-level candidates per candidate seen at each depth (emit_chunk_cap)
     uint32_t *tup[MAXQ];
     unsigned long long cap[MAXQ];
     uint32_t *cstart[MAXQ];
@@ -725,7 +735,8 @@ __device__ void ctl_plan(Ctl &c) {
         const double allowed = (double)c.cap[d] / fmax((double)c.ratio[d], 1.0 / 8192.0);
         const unsigned long long lim = (unsigned long long)fmax(allowed, (double)c.tile);
         if (chunk > lim) chunk = lim;
-        if (chunk > kMaxEmitChunk) chunk = kMaxEmitChunk;
+        const unsigned long long ncap = emit_chunk_cap((double)c.nxt[d]);
+        if (chunk > ncap) chunk = ncap;
     }
     StepArgs &a = c.args;
     a.depth = d;
@@ -782,6 +793,8 @@ __device__ void ctl_after(Ctl &c) {
     if (c.emits && (n > c.cap[d] || ovf)) {
         c.retries++;
         c.ratio[d] = (float)fmax((double)c.ratio[d] * 4.0, 2.0 * (double)n / (double)c.chunk);
+        if (ovf)  // the next level's candidates overflowed the field: at most half this chunk next
+            c.nxt[d] = (float)fmax((double)c.nxt[d] * 4.0, (double)kAllocMask / (double)c.chunk);
         return;
     }
     c.accepted = 1;
@@ -800,6 +813,7 @@ __device__ void ctl_after(Ctl &c) {
         for (uint32_t i = 0; i <= d; ++i) live += c.held[i] * tuple_bytes(i);
         if (live > c.peak) c.peak = live;
         c.ratio[d] = (float)fmax(2.0 * (double)n / (double)c.chunk, (double)c.ratio[d] * 0.5);
+        c.nxt[d] = (float)fmax((double)next / (double)c.chunk, (double)c.nxt[d] * 0.5);
         if (n > 0 && next > 0) {
             c.np[d + 1] = n;
             c.total[d + 1] = next;
@@ -1651,6 +1665,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0), held(dmax + 1, 0);
     std::vector<double> ratio(dmax + 1, ratio_init);
+    std::vector<double> nxt(dmax + 1, 0.0);  // next-level candidates per candidate seen (emit_chunk_cap)
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) has_final[q.k - 1] = 1;
     total[0] = root_total;
@@ -1668,7 +1683,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         if (emits) {
             const double allowed = (double)buf[d].cap / std::max(ratio[d], 1.0 / 8192.0);
             chunk = std::min<unsigned long long>(chunk, (unsigned long long)std::max<double>(allowed, TILE));
-            chunk = std::min<unsigned long long>(chunk, kMaxEmitChunk);
+            chunk = std::min<unsigned long long>(chunk, emit_chunk_cap(nxt[d]));
         }
         const uint32_t vtile = variant_tile(variant);
         chunk = std::min<unsigned long long>(chunk, (unsigned long long)dir_tiles * vtile);
@@ -1738,6 +1753,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             // candidates than the allocator indexes): redo a smaller chunk
             st.retries++;
             ratio[d] = std::max(ratio[d] * 4.0, 2.0 * (double)r.n_children / (double)chunk);
+            if (r.next_ovf)  // the next level's candidates overflowed the field: at most half this chunk next
+                nxt[d] = std::max(nxt[d] * 4.0, (double)kAllocMask / (double)chunk);
             continue;
         }
         if (trace)
@@ -1763,6 +1780,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
             st.peak_frontier_bytes = std::max<uint64_t>(st.peak_frontier_bytes, live);
             const double obs = (double)r.n_children / (double)chunk;
             ratio[d] = std::max(2.0 * obs, ratio[d] * 0.5);
+            nxt[d] = std::max((double)r.total_next / (double)chunk, nxt[d] * 0.5);
             if (r.n_children > 0 && r.total_next > 0) {
                 np[d + 1] = r.n_children;
                 total[d + 1] = r.total_next;

@@ -130,11 +130,17 @@ struct StepResult {
     unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
 };
 
-constexpr int kAllocShift = 38;                                  // child count: bits 38..63
-constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candidates: bits 0..37
+constexpr int kAllocShift = 36;                                  // child count: bits 36..63
+constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candidates: bits 0..35
 // An emitting step takes fewer candidates than the child-count field holds,
-// so the count never wraps (every candidate yields at most one child).
+// so the count never wraps (every candidate yields at most one child); a
+// step whose children's next-level candidates pass 2^36 raises next_ovf and
+// is re-run smaller.  The schedule sizes a depth's steps so that the next
+// level's candidates, at the rate observed there, fill at most half the
+// field; a depth's first step (rate not yet seen) takes at most
+// kFirstEmitChunk candidates.
 constexpr unsigned long long kMaxEmitChunk = (1ull << (64 - kAllocShift)) - 1024;
+constexpr unsigned long long kFirstEmitChunk = 1ull << 26;
 
 // Error bits of a schedule (the graph-driven controller sets them; the
 // host-driven loop checks the same conditions on the host).
