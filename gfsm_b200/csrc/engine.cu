@@ -78,21 +78,6 @@ struct GraphView {
 // searched in registers instead of by a chain of dependent probes.
 constexpr uint32_t SHORT_ROW = 8;
 
-// Entries of the row a[0, n), n <= SHORT_ROW, below k1 and below k2: one
-// pass, the loads independent of each other.
-__device__ __forceinline__ void short_bounds(const uint32_t *__restrict__ a, uint32_t n, uint32_t k1, uint32_t k2,
-                                             uint32_t &r1, uint32_t &r2) {
-    r1 = 0;
-    r2 = 0;
-#pragma unroll
-    for (uint32_t i = 0; i < SHORT_ROW; ++i)
-        if (i < n) {
-            const uint32_t x = __ldg(a + i);
-            r1 += x < k1;
-            r2 += x < k2;
-        }
-}
-
 // reqExists (HnGPU.cu:34-52) as a search: does the row adj[rs, re) hold
 // (v, lab)?
 __device__ __forceinline__ bool row_holds(const GraphView &g, uint32_t rs, uint32_t re, uint32_t v, uint32_t lab) {
@@ -149,7 +134,16 @@ struct StepArgs {
     const uint32_t *__restrict__ fan_list;
 };
 
+// A tuple's column 0: its trie node (bits 0-21) with flags.  kBranch: the
+// node has several child nodes (fan_list).  Bits 22-29: entries of the
+// tuple's next-level slice (bit i = entry i) that are vertices of the tuple
+// itself -- they would fail injectivity, so they are not candidates.
+// kInjDone: that set is complete (the slice came from a short row), so the
+// next level need not compare its candidates with the tuple again.
 constexpr uint32_t kBranch = 1u << 31;
+constexpr uint32_t kInjDone = 1u << 30;
+constexpr uint32_t kExclShift = 22;
+constexpr uint32_t kNodeMask = (1u << kExclShift) - 1u;
 
 // Also zeroes the step's per-query count scratch: final-level counts of a
 // step are added to the totals only once the host accepts the step, so a step
@@ -333,24 +327,45 @@ __device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, 
         khi = min(khi, x);
     }
     uint32_t s = rs, e = re;  // the part of w's row inside that window
+    uint32_t excl = 0, flags = 0;
     if (klo >= khi) {
         e = s;
     } else if (re - rs <= SHORT_ROW) {
-        uint32_t b1, b2;
-        short_bounds(a.g.adj + rs, re - rs, klo, khi, b1, b2);
+        // the row in registers: the window's bounds in one pass, and the
+        // slice entries that are vertices of the child's tuple (v and the
+        // parent's positions): they would fail injectivity at depth+1
+        // (HnGPU.cu:223-236) and are left out of its candidates
+        const uint32_t n = re - rs;
+        uint32_t b1 = 0, b2 = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < SHORT_ROW; ++i)
+            if (i < n) {
+                const uint32_t x = __ldg(a.g.adj + rs + i);
+                b1 += x < klo;
+                b2 += x < khi;
+            }
         s = rs + b1;
         e = rs + b2;
+        for (uint32_t i = 0; i < b2 - b1; ++i) {
+            const uint32_t x = __ldg(a.g.adj + s + i);
+            bool in = x == v;
+            for (uint32_t t = 0; t < d && !in; ++t) in = __ldg(a.ptup + (uint64_t)(1 + t) * a.pstride + p) == x;
+            excl |= (in ? 1u : 0u) << i;
+        }
+        flags = kInjDone;
     } else {
         if (klo) s = rs + lower_bound_u32(a.g.adj + rs, re - rs, klo);
         if (khi < a.g.n) e = rs + lower_bound_u32(a.g.adj + rs, re - rs, khi);
     }
     if (e <= s) return false;
+    const uint32_t len = (e - s) - __popc(excl);
+    if (!len) return false;  // every entry of the slice is a vertex of the tuple
     // a branching node's child offers its slice to every child node
     const uint32_t nf = L->fan_count;
     const uint32_t mult = nf > 1 ? nf : 1u;
     r.cs = s;
-    r.cnt = (e - s) * mult;
-    r.q = nf > 1 ? (q | kBranch) : q;
+    r.cnt = len * mult;
+    r.q = q | (excl << kExclShift) | flags | (nf > 1 ? kBranch : 0u);
     // the child's tuple and anchor row, read once per (member) parent
     my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
     return true;
@@ -380,17 +395,28 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
     const unsigned long long pc = t.win ? t.win[lo] : __ldg(a.pcoff + p);
     uint32_t local = (uint32_t)(c - pc);
     uint32_t q = ROOT ? __ldg(a.root_rep + p) : __ldg(a.ptup + p);
+    const uint32_t excl = ROOT ? 0u : (q >> kExclShift) & 0xffu;
+    const bool inj_done = !ROOT && (q & kInjDone);
     if (!ROOT && (q & kBranch)) {
         // the parent's trie node branches: its candidates run over (child
         // node, row offset), one copy of its slice per child node
-        q &= ~kBranch;
+        q &= kNodeMask;
         const DLevel *P = &a.plans[q].lv[d - 1];
         const unsigned long long pn = t.win ? t.win[lo + 1] : __ldg(a.pcoff + p + 1);
         const uint32_t slen = (uint32_t)(pn - pc) / P->fan_count;  // the fan-out cap keeps pn - pc < 2^32
         const uint32_t j = local / slen;
         local -= j * slen;
         q = __ldg(a.fan_list + P->fan_start + j);
+    } else if (!ROOT) {
+        q &= kNodeMask;
     }
+    // the parent's first candidate (of each child node) does the parent's
+    // byte accounting below
+    const bool acct = !ROOT && local == 0;
+    // row offset of the local-th slice entry that is not left out (excl,
+    // ascending positions)
+    for (uint32_t m = excl; m; m &= m - 1u)
+        if ((uint32_t)(__ffs(m) - 1) <= local) ++local;
     const DLevel *L = &a.plans[q].lv[d];
     uint32_t v;
     bool pass = true;
@@ -404,16 +430,17 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
             pass = has_edge(a.g, __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
         else if (a.g.elab)
             pass = __ldg(a.g.elab + idx) == L->anchor_lab;
-        // injectivity (HnGPU.cu:223-236)
-        for (uint32_t i = 0; i < d; ++i)
-            if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
+        // injectivity (HnGPU.cu:223-236), unless the parent's slice already
+        // left out every vertex of its tuple
+        if (!inj_done)
+            for (uint32_t i = 0; i < d; ++i)
+                if (__ldg(a.ptup + (uint64_t)(1 + i) * a.pstride + p) == v) pass = false;
     }
     // Algorithmic bytes of a parent (its tuple, its anchor row and every
     // requirement row, each read once): the tuple and anchor-row terms were
     // added when the parent was written (below, where the anchor row's bounds
     // are at hand); the parent's first candidate adds its requirement rows
     // here, from the same row bounds the requirement checks load.
-    const bool acct = !ROOT && local == 0;
     // remaining requirements (HnGPU.cu:243-252)
     for (uint32_t r = 0; r < L->nreq && (pass || acct); ++r) {
         const uint32_t mode = (t.single && r < (uint32_t)NSTAGE) ? t.rmode[r] : 0u;
@@ -487,9 +514,10 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
 
     // ---- a tile inside one parent's slice (hub rows): stage the part of each
     // requirement row that can hold this tile's candidates
-    const bool single = !ROOT && plo == phi && a.g.elab == nullptr && !(__ldg(a.ptup + plo) & kBranch);
+    const bool single = !ROOT && plo == phi && a.g.elab == nullptr &&
+                        !(__ldg(a.ptup + plo) & (kBranch | (0xffu << kExclShift)));
     if (single) {
-        const uint32_t q0 = __ldg(a.ptup + plo);
+        const uint32_t q0 = __ldg(a.ptup + plo) & kNodeMask;
         const DLevel *L0 = &a.plans[q0].lv[d];
         if (tid == 0) {
             const uint32_t cs0 = __ldg(a.pcstart + plo);
@@ -519,7 +547,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
         }
     }
-    if (tid == 0) sm.q0 = ROOT ? __ldg(a.root_rep + plo) : (__ldg(a.ptup + plo) & ~kBranch);
+    if (tid == 0) sm.q0 = ROOT ? __ldg(a.root_rep + plo) : (__ldg(a.ptup + plo) & kNodeMask);
     __syncthreads();
 
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
@@ -1350,6 +1378,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
     }
     const uint32_t na = (uint32_t)active.size();
+    if (na > kNodeMask) {  // a tuple's trie node id has 22 bits
+        err = "a call takes at most " + std::to_string(kNodeMask) + " queries";
+        return GFSM_ERR_TOO_LARGE;
+    }
     if (na == 0) {
         if (stats) {
             st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
