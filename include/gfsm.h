@@ -230,7 +230,8 @@ gfsm_status gfsm_match_mappings(gfsm_ctx *ctx, const gfsm_plan *plan, const gfsm
  * (max_candidates) of data's context. */
 gfsm_status gfsm_match_count_noalloc(const gfsm_plan *plan, const gfsm_graph *data, void *stream,
                                      uint64_t *count);
-/* Many queries against one resident data graph in one device pass. */
+/* Many queries against one resident data graph in one device pass (at most
+ * 4,194,303 queries per call; more return GFSM_ERR_TOO_LARGE). */
 gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq,
                              const gfsm_graph *data, uint64_t *counts, gfsm_stats *stats);
 
