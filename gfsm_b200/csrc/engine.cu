@@ -132,6 +132,10 @@ struct StepArgs {
     // kBranch set when the node has several child nodes (fan_list)
     const uint32_t *__restrict__ root_rep;
     const uint32_t *__restrict__ fan_list;
+    // count a last query vertex when its parent is written, where nothing is
+    // left to check (next_slice); only where the step's counts are committed
+    // after the step is accepted (a re-run step must not count twice)
+    uint32_t leaf_count;
 };
 
 // A tuple's column 0: its trie node (bits 0-21) with flags.  kBranch: the
@@ -307,7 +311,7 @@ struct CandCtx {
 // False when the slice is empty -- such a child cannot be extended and is
 // not written.
 __device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, Stage &r,
-                                           unsigned long long &my_bytes) {
+                                           unsigned long long &my_bytes, uint32_t &fq, unsigned long long &fc) {
     const uint32_t p = r.p, v = r.v, q = r.q;
     const DLevel *L = &a.plans[q].lv[d];
     const uint32_t na = L->next_anchor;
@@ -363,11 +367,27 @@ __device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, 
     // a branching node's child offers its slice to every child node
     const uint32_t nf = L->fan_count;
     const uint32_t mult = nf > 1 ? nf : 1u;
+    // the child's tuple and anchor row, read once per (member) parent
+    my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
+    if (a.leaf_count && flags && nf <= 1 && !a.g.elab) {
+        // depth+1 is the last query vertex with nothing to check beyond the
+        // anchor edge (no requirement, no row search for the anchor): every
+        // entry left in the slice is an embedding -- count them here and
+        // write no child
+        const DLevel *N = &a.plans[q].lv[d + 1];
+        if (N->final_ && N->nreq == 0 && !N->anchor_check) {
+            if (fc && q != fq) {
+                atomicAdd(&a.counts[fq], fc);
+                fc = 0;
+            }
+            fq = q;
+            fc += len;
+            return false;
+        }
+    }
     r.cs = s;
     r.cnt = len * mult;
     r.q = q | (excl << kExclShift) | flags | (nf > 1 ? kBranch : 0u);
-    // the child's tuple and anchor row, read once per (member) parent
-    my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
     return true;
 }
 
@@ -583,7 +603,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
             bool keep = false;
             if (e < wcnt) {
                 r = wstage[e];
-                keep = next_slice(a, d, r, my_bytes);
+                keep = next_slice(a, d, r, my_bytes, fq, fc);
             }
             const uint32_t bal = __ballot_sync(0xffffffffu, keep);
             if (keep) wstage[kept + __popc(bal & ((1u << lane) - 1u))] = r;
@@ -1602,6 +1622,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     // chunk (default 1: a first chunk never overflows).  A smaller guess takes
     // larger first chunks -- fewer steps where survival is low, re-runs where
     // it is not.  Later chunks follow the observed ratio either way.
+    // last query vertices counted when their parents are written (next_slice):
+    // not when mappings are captured (such a vertex gets no row)
+    const bool leaf_ok = !rows_out;
     const double ratio_init = [] {  // read per call: cheap, and tests change it
         const char *v = getenv("GFSM_SURVIVOR_GUESS");
         const double x = v && *v ? atof(v) : 1.0;
@@ -1650,6 +1673,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_ctr = rows_ctr;
         a.root_rep = d_root_rep;
         a.fan_list = d_fan_list;
+        a.leaf_count = leaf_ok ? 1u : 0u;
         Ctl *d_ctl = static_cast<Ctl *>(ctl);
         ECHECK(cudaMemcpyAsync(d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         st.h2d_bytes += sizeof(Ctl);
@@ -1699,7 +1723,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     std::vector<double> ratio(dmax + 1, ratio_init);
     std::vector<double> nxt(dmax + 1, 0.0);  // next-level candidates per candidate seen (emit_chunk_cap)
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
-    for (const DQuery &q : dq) has_final[q.k - 1] = 1;
+    for (const DQuery &q : dq) {
+        has_final[q.k - 1] = 1;
+        if (leaf_ok && q.k >= 2) has_final[q.k - 2] = 1;  // last vertices counted when their parents are written
+    }
     total[0] = root_total;
     np[0] = nr;
     uint32_t d = 0;
@@ -1754,6 +1781,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         a.rows_ctr = rows_ctr;
         a.root_rep = d_root_rep;
         a.fan_list = d_fan_list;
+        a.leaf_count = leaf_ok ? 1u : 0u;
         a.pcoff_end = total[d];
         k_partition<<<(unsigned)div_up((uint64_t)std::max<uint32_t>(ntiles + 1, ne), 256), 256, 0, stream>>>(
             a.pcoff, a.np, a.pcoff_end, a.c0, chunk, ntiles, vtile, tile_parent, d_result, d_step_counts, ne);
