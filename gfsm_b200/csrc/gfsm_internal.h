@@ -130,11 +130,11 @@ struct StepResult {
     unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
 };
 
-constexpr int kAllocShift = 36;                                  // child count: bits 36..63
-constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candidates: bits 0..35
+constexpr int kAllocShift = 34;                                  // child count: bits 34..63
+constexpr unsigned long long kAllocMask = (1ull << kAllocShift) - 1;  // candidates: bits 0..33
 // An emitting step takes fewer candidates than the child-count field holds,
 // so the count never wraps (every candidate yields at most one child); a
-// step whose children's next-level candidates pass 2^36 raises next_ovf and
+// step whose children's next-level candidates pass 2^34 raises next_ovf and
 // is re-run smaller.  The schedule sizes a depth's steps so that the next
 // level's candidates, at the rate observed there, fill at most half the
 // field; a depth's first step (rate not yet seen) takes at most
