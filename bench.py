@@ -513,17 +513,23 @@ def run_ours(args, rank, world, local, pg):
         tpath = os.path.join(tempfile.mkdtemp(), "grid.g")
         g.write_text(tpath)
         size = os.path.getsize(tpath)
-        t0 = time.perf_counter()
-        tg = ctx.file_parse(tpath)
-        t1 = time.perf_counter()
-        tg.to_device()
-        t2 = time.perf_counter()
-        bi = tg.info()
-        ingest = {"bytes": size, "parse_s": t1 - t0, "device_build_s": t2 - t1,
+        runs = []  # three parse + build rounds; the median round is reported (the host is shared)
+        for _ in range(3):
+            t0 = time.perf_counter()
+            tg = ctx.file_parse(tpath)
+            t1 = time.perf_counter()
+            tg.to_device()
+            t2 = time.perf_counter()
+            runs.append((t2 - t1, t1 - t0, tg.info()))
+            tg.close()
+        runs.sort(key=lambda r: r[0])
+        build_s, parse_s, bi = runs[1]
+        ingest = {"bytes": size, "parse_s": sorted(r[1] for r in runs)[1], "device_build_s": build_s,
+                  "device_build_s_runs": [round(r[0], 4) for r in runs],
                   "device_build_split_ms": {k: bi["build_" + k + "_ms"] for k in ("alloc", "h2d", "kernel", "d2h",
                                                                                    "wall")},
-                  "parse_mb_per_s": size / (t1 - t0) / 1e6, "threads": os.cpu_count()}
-        tg.close()
+                  "parse_mb_per_s": size / sorted(r[1] for r in runs)[1] / 1e6, "threads": os.cpu_count(),
+                  "note": "median of three parse + device-build rounds of the same text"}
         os.unlink(tpath)
     import torch
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
