@@ -668,7 +668,8 @@ def run_ours(args, rank, world, local, pg):
     k_launches = step_launches
     traffic = None
     if tr and k_launches:
-        # measured DRAM bytes per candidate (small-case ncu capture) x candidates per launch
+        # DRAM bytes per candidate measured over a full-size batch (profiles/traffic.json)
+        # x the candidates of an average level-step launch
         traffic = tr["dram_bytes_per_candidate"] * cand / k_launches
     roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
