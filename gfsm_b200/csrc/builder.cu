@@ -314,6 +314,24 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
         if (d) out.rows++;
         out.max_degree = std::max(out.max_degree, d);
     }
+    {
+        // the degree window of every (label group, degree bound < 17): a
+        // query vertex's degree bound is below its query's size (at most 16)
+        const uint32_t ng = (uint32_t)out.group_value.size(), K = DeviceGraph::kCutDeltas;
+        out.deg_cut.assign((size_t)ng * K, 0);
+        for (uint32_t gi = 0; gi < ng; ++gi) {
+            const uint32_t glo = out.group_start[gi], ghi = out.group_start[gi + 1];
+            out.deg_cut[(size_t)gi * K] = ghi;  // delta 0: the whole group
+            for (uint32_t delta = 1; delta < K; ++delta) {
+                uint32_t a = glo, b = ghi;  // ids are degree-descending inside the group
+                while (a < b) {
+                    const uint32_t mid = a + (b - a) / 2;
+                    if (out.h_rowptr[mid + 1] - out.h_rowptr[mid] >= delta) a = mid + 1; else b = mid;
+                }
+                out.deg_cut[(size_t)gi * K + delta] = a;
+            }
+        }
+    }
     out.bytes = ((uint64_t)n + 1) * 4 + m * 4 + (out.elab ? m : 0) + (uint64_t)n * 4;
     out.build_wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
 

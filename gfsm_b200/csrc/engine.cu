@@ -980,13 +980,14 @@ gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits 
     std::vector<uint32_t> lo(k), hi(k);
     for (uint32_t d = 0; d < k; ++d) {
         uint32_t glo = 0, ghi = g.n;
+        size_t gsel = 0;  // the depth's vertex-label group (group 0: labels not matched)
         if (g.vl_grouped) {
             auto it = std::lower_bound(g.group_value.begin(), g.group_value.end(), p.qlabel[d]);
             if (it == g.group_value.end() || *it != p.qlabel[d]) { never = true; glo = ghi = 0; }
             else {
-                size_t gi = (size_t)(it - g.group_value.begin());
-                glo = g.group_start[gi];
-                ghi = g.group_start[gi + 1];
+                gsel = (size_t)(it - g.group_value.begin());
+                glo = g.group_start[gsel];
+                ghi = g.group_start[gsel + 1];
             }
         }
         // degree window: ids in a group are degree-descending, so
@@ -994,13 +995,17 @@ gfsm_status build_dquery(const Plan &p, const DeviceGraph &g, const gfsm_limits 
         uint32_t delta = use_deg ? p.qdeg[d] : 0;
         if (d == 0) delta = std::max<uint32_t>(delta, 1);  // a root needs a CCSR row (HnGPU.cu:475-495)
         uint32_t cut = ghi;
-        if (delta > 0) {
-            uint32_t a = glo, b = ghi;
-            while (a < b) {
-                uint32_t mid = a + (b - a) / 2;
-                if (g.degree(mid) >= delta) a = mid + 1; else b = mid;
+        if (delta > 0 && glo < ghi) {
+            if (delta < DeviceGraph::kCutDeltas && !g.deg_cut.empty()) {
+                cut = g.deg_cut[gsel * DeviceGraph::kCutDeltas + delta];
+            } else {
+                uint32_t a = glo, b = ghi;
+                while (a < b) {
+                    uint32_t mid = a + (b - a) / 2;
+                    if (g.degree(mid) >= delta) a = mid + 1; else b = mid;
+                }
+                cut = a;
             }
-            cut = a;
         }
         lo[d] = glo;
         hi[d] = cut;
@@ -1280,7 +1285,7 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
         return v >= 0 && v < kVariants ? v : 0;
     }
     const char *at = getenv("GFSM_AUTOTUNE");
-    if (!autotune || (at && *at == '0')) return 0;
+    if (at && *at == '0') return 0;
     uint32_t kmax = 0;
     for (const Plan *p : plans) kmax = std::max(kmax, p->k);
     const double avg = g.n ? (double)g.m / (double)g.n : 0.0;
@@ -1288,6 +1293,21 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
                          (uint64_t)std::lround(std::log2((double)plans.size() + 1.0));
     auto it = tuned.find(key);
     if (it != tuned.end()) return it->second;
+    if (!autotune) {
+        // no tuning runs here (served slots): the choice already made for the
+        // nearest batch size of the same workload class, else the default
+        int best = 0;
+        long dist = -1;
+        for (const auto &kv : tuned)
+            if ((kv.first >> 8) == (key >> 8)) {
+                const long dd = std::labs((long)(kv.first & 0xff) - (long)(key & 0xff));
+                if (dist < 0 || dd < dist) {
+                    dist = dd;
+                    best = kv.second;
+                }
+            }
+        return best;
+    }
     // The sample is the call's first 32 queries, grown fourfold (up to 2,048)
     // while the default geometry takes under 2 ms on it: shorter samples are
     // launch-bound and their timings mostly noise.  Another geometry must

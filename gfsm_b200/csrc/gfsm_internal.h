@@ -52,6 +52,11 @@ struct DeviceGraph {
     std::vector<uint32_t> h_order;    // [n]
     std::vector<uint32_t> group_value;// sorted distinct vertex label values (grouped mode)
     std::vector<uint32_t> group_start;// [groups+1]
+    // degree windows: deg_cut[g * kCutDeltas + delta] = the first id of
+    // group g whose degree is below delta (ids in a group are
+    // degree-descending), for delta < kCutDeltas
+    static constexpr uint32_t kCutDeltas = 17;
+    std::vector<uint32_t> deg_cut;
     uint64_t bytes = 0;
     // build time: allocation, host-to-device copies, device passes, copies
     // back (CUDA events on the build stream), and the host wall time

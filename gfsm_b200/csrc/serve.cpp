@@ -26,6 +26,8 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr uint64_t kAdmitArenas = 8;  // default admission budget, in slot arenas
+
 struct Req {
     uint64_t id;
     Plan plan;
@@ -187,7 +189,10 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         rc = e->init(ctx->device, 0, scan, err);
         if (rc != GFSM_OK) return rc;
         e->arena_cap = per_slot > e->small_bytes ? per_slot - e->small_bytes : 0;
-        e->autotune = false;  // a request never waits for tuning runs
+        e->autotune = false;  // a request never waits for tuning runs ...
+        // ... but a slot uses the tile geometries the context's own engine
+        // has already chosen (batched calls on the same context)
+        if (ctx->engine) e->tuned = static_cast<Engine *>(ctx->engine)->tuned;
         // pinned staging for a full batch's plans, so no request allocates it
         const uint64_t stage = std::max<uint64_t>(1ull << 20, (uint64_t)c.max_batch * sizeof(DQuery) * 2);
         if (cudaMallocHost(&e->h_stage, stage) != cudaSuccess) return GFSM_ERR_NOMEM;
@@ -202,7 +207,12 @@ gfsm_status gfsm_serve_start(gfsm_ctx *ctx, const gfsm_graph *data, const gfsm_s
         if (rc != GFSM_OK) return rc;
         s->engines.push_back(std::move(e));
     }
-    s->slot_budget = c.frontier_bytes ? c.frontier_bytes : per_slot;
+    // default admission budget: 8 arenas' worth of predicted (unchunked)
+    // frontier -- the engine's depth-first chunking runs such a batch in its
+    // own arena with a few more steps, while a budget of one arena split
+    // saturated batches into a few hundred queries and lost the shared
+    // prefixes (40k offered queries/s on the road grid: 28k -> see the bench)
+    s->slot_budget = c.frontier_bytes ? c.frontier_bytes : kAdmitArenas * per_slot;
     s->t0 = Clock::now();
     gfsm_server *raw = s.get();
     for (int i = 0; i < c.slots; ++i) s->workers.emplace_back([raw, i] { raw->worker(i); });

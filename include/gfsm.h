@@ -112,7 +112,8 @@ typedef struct {
     int32_t  slots;              /* concurrent device batches (streams), default 2   */
     int32_t  max_batch;          /* queries per device batch, default 256            */
     int32_t  queue_capacity;     /* pending requests, default 65536                  */
-    uint64_t frontier_bytes;     /* admission budget per slot; 0 = mem_limit / slots */
+    uint64_t frontier_bytes;     /* admission budget per slot (sum of the batch's predicted
+                                    frontier bytes); 0 = 8 x mem_limit / slots */
 } gfsm_serve_config;
 
 /* --- context ----------------------------------------------------------- */
