@@ -40,7 +40,6 @@
 #include <map>
 #include <mutex>
 #include <thread>
-#include <unordered_map>
 
 #include "engine.h"
 
@@ -1418,6 +1417,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
     }
     const uint32_t na = (uint32_t)active.size();
+    const auto t_plans = std::chrono::steady_clock::now();
     if (na > kNodeMask) {  // a tuple's trie node id has 22 bits
         err = "a call takes at most " + std::to_string(kNodeMask) + " queries";
         return GFSM_ERR_TOO_LARGE;
@@ -1456,8 +1456,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     if (share) {
         // members of a node grouped by their plan at depth d (hash of the
         // 64 plan bytes, equality checked bytewise), each group's members
-        // ascending, groups ordered by representative -- the first member
-        // seen, as members arrive ascending
+        // ascending, groups ordered by representative (smallest member)
         auto lv_hash = [&](uint32_t i, uint32_t d) {
             uint64_t w[sizeof(DLevel) / 8];
             std::memcpy(w, &dq[i].lv[d], sizeof(DLevel));
@@ -1467,24 +1466,35 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         };
         auto split = [&](const std::vector<uint32_t> &mem, uint32_t d) {
             std::vector<std::vector<uint32_t>> out;
-            std::unordered_multimap<uint64_t, uint32_t> by;  // hash -> group
-            by.reserve(mem.size() * 2);
-            for (uint32_t i : mem) {
-                const uint64_t h = lv_hash(i, d);
-                uint32_t gi = ~0u;
-                auto rg = by.equal_range(h);
-                for (auto it = rg.first; it != rg.second; ++it)
-                    if (!std::memcmp(&dq[out[it->second][0]].lv[d], &dq[i].lv[d], sizeof(DLevel))) {
-                        gi = it->second;
-                        break;
-                    }
-                if (gi == ~0u) {
-                    gi = (uint32_t)out.size();
-                    out.emplace_back();
-                    by.emplace(h, gi);
-                }
-                out[gi].push_back(i);
+            if (mem.size() == 1) {
+                out.push_back(mem);
+                return out;
             }
+            // members sorted by (plan hash, id): a run of equal hashes holds
+            // one group per distinct plan (compared bytewise), each group's
+            // members ascending; then the groups by representative
+            std::vector<std::pair<uint64_t, uint32_t>> hv(mem.size());
+            for (size_t i = 0; i < mem.size(); ++i) hv[i] = {lv_hash(mem[i], d), mem[i]};
+            std::sort(hv.begin(), hv.end());
+            for (size_t i = 0; i < hv.size();) {
+                size_t j = i;
+                while (j < hv.size() && hv[j].first == hv[i].first) ++j;
+                const size_t run0 = out.size();
+                for (size_t t = i; t < j; ++t) {
+                    const uint32_t m = hv[t].second;
+                    size_t gi = out.size();
+                    for (size_t g2 = run0; g2 < out.size(); ++g2)
+                        if (!std::memcmp(&dq[out[g2][0]].lv[d], &dq[m].lv[d], sizeof(DLevel))) {
+                            gi = g2;
+                            break;
+                        }
+                    if (gi == out.size()) out.emplace_back();
+                    out[gi].push_back(m);
+                }
+                i = j;
+            }
+            std::sort(out.begin(), out.end(),
+                      [](const std::vector<uint32_t> &a, const std::vector<uint32_t> &b) { return a[0] < b[0]; });
             return out;
         };
         std::vector<uint32_t> all(na);
@@ -1525,6 +1535,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         for (uint32_t i = 0; i < na; ++i) root_rep.push_back(i);
     const uint32_t ne = na;                        // count slots: one per query (representatives)
     const uint32_t nr = (uint32_t)root_rep.size();  // root-level parents
+    const auto t_trie = std::chrono::steady_clock::now();
     if (fan_list.empty()) fan_list.push_back(0);
 
     // arena layout: plans | counts | step counts | root coff | root cstart |
@@ -1601,6 +1612,13 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
         return out;
     };
+    if (trace) {
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        fprintf(stderr, "gfsm-host plans=%.3f trie=%.3f staging=%.3f ms (queries %u, root nodes %u)\n",
+                ms(t_start, t_plans), ms(t_plans, t_trie), ms(t_trie, std::chrono::steady_clock::now()), na, nr);
+    }
     ECHECK(cudaEventRecord(ev_begin, stream));
 
     // depth buffers 0 .. dmax-1 (depth dmax is count-only)
