@@ -714,7 +714,7 @@ def run_ours(args, rank, world, local, pg):
             "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": dict(config_for(args.queries, world), mem_limit=mem),
+            "config": config_for(args.queries, world), "mem_limit": mem,
             "exact": exact, "exact_vs_oracle": exact_vs_oracle,
             "exact_note": "batched == plain == served on every query; every batched count equals the "
                           "oracle's (tests/golden/bench_cfg5_counts.json, all queries); the CPU legs "
