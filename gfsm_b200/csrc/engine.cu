@@ -921,20 +921,29 @@ __global__ void k_part_g(const Ctl *ctl) {
 }
 
 // Graph nodes: the level step on a fixed grid; every CTA takes tiles from
-// the step's tile queue.  One instantiation per argument slot, tile geometry
-// and step kind: the root step and the deeper levels are separate nodes, and
-// the one whose kind the step is not returns at once (one kernel holding both
-// had twice the code and spilled).
+// the step's tile counter (StepResult::tile_ctr, zeroed with the result by
+// the tile directory), so tiles go to whichever CTA frees first, as they
+// would with one CTA per tile.  The ticket for a CTA's next tile is taken
+// when its current tile starts and read when it ends, so the atomic's round
+// trip hides behind the tile.  One instantiation per argument slot, tile
+// geometry and step kind: the root step and the deeper levels are separate
+// nodes, and the one whose kind the step is not returns at once (one kernel
+// holding both had twice the code and spilled).
 template <int SLOT, class G, bool ROOT>
 __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
     __shared__ StepSmem<G> sm;
+    __shared__ uint32_t s_tile;
     const StepArgs &a = c_args[SLOT];
     if ((a.depth == 0) != ROOT) return;
-    // tiles are dealt out grid-stride: a shared tile counter taken with an
-    // atomic per tile stalled every tile's start on an address all resident
-    // CTAs contend for (grid batch 132 ms against 115 ms of separate launches)
-    for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        step_tile<ROOT, G>(a, tile, sm);
+    if (threadIdx.x == 0) s_tile = atomicAdd(&a.result->tile_ctr, 1u);
+    __syncthreads();
+    for (;;) {
+        const uint32_t tile = s_tile;
+        if (tile >= a.ntiles) break;
+        uint32_t next = 0;
+        if (threadIdx.x == 0) next = atomicAdd(&a.result->tile_ctr, 1u);
+        step_tile<ROOT, G>(a, tile, sm);  // its barriers order every thread's read of s_tile before the write
+        if (threadIdx.x == 0) s_tile = next;
         __syncthreads();
     }
 }

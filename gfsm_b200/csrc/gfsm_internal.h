@@ -131,7 +131,7 @@ struct StepResult {
     unsigned long long alloc;
     unsigned int err;          // error bits a kernel may raise (none does today; the host checks them)
     unsigned int rows;         // mapping rows claimed (mapping mode)
-    unsigned int pad;
+    unsigned int tile_ctr;     // graph-driven steps: tiles handed out so far (tickets)
     unsigned int next_ovf;     // the step's next-level candidates exceed the allocator's field
 };
 
