@@ -1285,6 +1285,17 @@ gfsm_status Engine::build_graph(int variant, std::string &err) {
 // batch size) -- by timing every geometry on a sample of the call's queries
 // the first time a class is seen.  GFSM_TILE=<0..3> forces a geometry and
 // GFSM_AUTOTUNE=0 keeps the default.
+// Workload class of a call (the autotuner's and the step sizer's memory key):
+// the largest query size, log2 of the data graph's average degree and log2
+// of the number of queries.
+static uint64_t workload_class(const std::vector<const Plan *> &plans, const DeviceGraph &g) {
+    uint32_t kmax = 0;
+    for (const Plan *p : plans) kmax = std::max(kmax, p->k);
+    const double avg = g.n ? (double)g.m / (double)g.n : 0.0;
+    return ((uint64_t)kmax << 16) | ((uint64_t)std::lround(std::log2(avg + 1.0)) << 8) |
+           (uint64_t)std::lround(std::log2((double)plans.size() + 1.0));
+}
+
 int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                          std::string &err) {
     const char *force = getenv("GFSM_TILE");
@@ -1294,11 +1305,7 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
     }
     const char *at = getenv("GFSM_AUTOTUNE");
     if (at && *at == '0') return 0;
-    uint32_t kmax = 0;
-    for (const Plan *p : plans) kmax = std::max(kmax, p->k);
-    const double avg = g.n ? (double)g.m / (double)g.n : 0.0;
-    const uint64_t key = ((uint64_t)kmax << 16) | ((uint64_t)std::lround(std::log2(avg + 1.0)) << 8) |
-                         (uint64_t)std::lround(std::log2((double)plans.size() + 1.0));
+    const uint64_t key = workload_class(plans, g);
     auto it = tuned.find(key);
     if (it != tuned.end()) return it->second;
     if (!autotune) {
@@ -1689,10 +1696,15 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         graph_driver = build_graph(variant, gerr) == GFSM_OK;
         if (!graph_driver) st.graph_error = last_graph_error ? last_graph_error : -1;
     }
+    // next-level candidates per candidate each depth saw in this workload
+    // class's last call: the first step of a depth is sized from it
+    std::vector<double> &seen = nxt_seen[workload_class(plans, g)];
+    if (seen.size() < (size_t)dmax + 1) seen.resize((size_t)dmax + 1, 0.0);
     if (graph_driver) {
         Ctl c;
         std::memset(&c, 0, sizeof(c));
         c.total[0] = root_total;
+        for (uint32_t i = 0; i <= dmax; ++i) c.nxt[i] = (float)seen[i];
         c.np[0] = nr;
         for (int i = 0; i <= MAXQ; ++i) c.ratio[i] = (float)ratio_init;
         for (uint32_t i = 0; i < dmax; ++i) {
@@ -1736,6 +1748,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         st.steps = c.steps;
+        for (uint32_t i = 0; i <= dmax; ++i) seen[i] = c.nxt[i];
         st.peak_frontier_bytes = c.peak;
         st.launches = (uint32_t)(1 + 4 * c.steps);  // first controller, then partition, root step, step, controller
         st.retries = c.retries;
@@ -1768,7 +1781,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     }
     std::vector<unsigned long long> total(dmax + 1, 0), pos(dmax + 1, 0), np(dmax + 1, 0), held(dmax + 1, 0);
     std::vector<double> ratio(dmax + 1, ratio_init);
-    std::vector<double> nxt(dmax + 1, 0.0);  // next-level candidates per candidate seen (emit_chunk_cap)
+    std::vector<double> nxt(seen.begin(), seen.begin() + dmax + 1);  // emit_chunk_cap's rates
     std::vector<char> has_final(dmax + 1, 0);  // some query ends at this depth
     for (const DQuery &q : dq) {
         has_final[q.k - 1] = 1;
@@ -1897,6 +1910,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
     }
     ECHECK(cudaEventRecord(ev_end, stream));
+    for (uint32_t i = 0; i <= dmax; ++i) seen[i] = nxt[i];
     std::vector<unsigned long long> ecnt(ne);
     ECHECK(cudaMemcpyAsync(ecnt.data(), d_counts, (uint64_t)ne * 8, cudaMemcpyDeviceToHost, stream));
     st.d2h_bytes += (uint64_t)ne * 8;

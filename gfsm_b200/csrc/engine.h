@@ -59,6 +59,10 @@ struct Engine {
     int pick_variant(const std::vector<const Plan *> &plans, const DeviceGraph &g, const gfsm_limits &lim,
                      std::string &err);
     std::map<uint64_t, int> tuned;  // autotuner: workload class -> tile geometry
+    // per workload class, the next-level candidates per candidate each depth
+    // saw in the last call: the next call sizes a depth's first step from it
+    // instead of the conservative first-step cap
+    std::map<uint64_t, std::vector<double>> nxt_seen;
     bool autotune = true;           // off for served slots: tuning runs would sit on the request path
 };
 
