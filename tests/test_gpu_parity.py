@@ -294,6 +294,33 @@ def test_device_and_host_drivers_agree(monkeypatch, tile):
     ctx.close()
 
 
+@pytest.mark.parametrize("driver", ["host", "graph"])
+def test_repeated_call_takes_larger_first_steps(monkeypatch, driver):
+    """A depth's first step is capped until its next-level rate is known; a
+    repeated call of the same workload class starts from the rates its
+    predecessor saw, so it needs no more steps, and counts, candidates and
+    expansions do not change."""
+    monkeypatch.setenv("GFSM_DRIVER", driver)
+    monkeypatch.setenv("GFSM_TILE", "0")
+    ctx = gfsm_b200.GFSM(device=0, vertex_labels=1)
+    g = synth.grid(700, 0.05, 0.02, seed=8)
+    g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=9)
+    s, d = g.directed()
+    data = ctx.graph_from_edges(g.n, s, d, None, g.vlabel)
+    plans = []
+    for i in range(64):
+        qg, _ = synth.rw_query(g, 4 + i % 4, tree=i % 2 == 0, seed=700 + i)
+        qs, qd = qg.directed()
+        plans.append(ctx.pre_process_query(ctx.graph_from_edges(qg.n, qs, qd, None, qg.vlabel)))
+    c1, s1 = ctx.batch_count(plans, data)
+    c2, s2 = ctx.batch_count(plans, data)
+    assert c1.tolist() == c2.tolist() and c1.sum() > 0
+    for key in ("candidates", "expansions"):
+        assert s1[key] == s2[key], key
+    assert s2["steps"] <= s1["steps"] and s2["retries"] == 0
+    ctx.close()
+
+
 def test_default_driver_policy(monkeypatch):
     """Without GFSM_DRIVER a call whose first level (the CCSR entries of its
     queries' root windows) holds at most 2^22 candidates runs on the graph,
