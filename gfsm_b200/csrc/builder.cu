@@ -214,6 +214,21 @@ gfsm_status build_device_graph(const HostGraph &h, int device, bool vl_mode, Dev
                                   n1 * 8, n1 * 8, m1 * 8, m1 * 8, tmp_bytes};
         uint64_t total = 0;
         for (uint64_t x : sizes) total += al(x);
+        // the device's default pool keeps up to 4 GiB of freed workspace
+        // reserved for this process (the pool releases everything at each
+        // synchronisation otherwise), so a second build does not map its
+        // workspace again: builds of the same graph measured 28 ms to 0.9 s
+        // with the mapping redone every time
+        {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+                uint64_t keep = 4ull << 30, cur = 0;
+                if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess &&
+                    cur < keep)
+                    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            cudaGetLastError();
+        }
         BCHECK(cudaMallocAsync(reinterpret_cast<void **>(&ws), total, st));
         char *w = ws;
         auto take = [&](uint64_t bytes) {
