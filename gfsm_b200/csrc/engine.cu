@@ -920,7 +920,8 @@ __global__ void k_part_g(const Ctl *ctl) {
     }
 }
 
-// Graph nodes: the level step on a fixed grid; every CTA takes tiles from
+// Graph nodes: the level step on a fixed grid.  A step with no more tiles
+// than CTAs gives each CTA its own tile; otherwise every CTA takes tiles from
 // the step's tile counter (StepResult::tile_ctr, zeroed with the result by
 // the tile directory), so tiles go to whichever CTA frees first, as they
 // would with one CTA per tile.  The ticket for a CTA's next tile is taken
@@ -934,7 +935,11 @@ __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
     __shared__ StepSmem<G> sm;
     __shared__ uint32_t s_tile;
     const StepArgs &a = c_args[SLOT];
-    if ((a.depth == 0) != ROOT) return;
+    if ((a.depth == 0) != ROOT || blockIdx.x >= a.ntiles) return;
+    if (a.ntiles <= gridDim.x) {  // a step that fits the grid: one tile per CTA, no tickets
+        step_tile<ROOT, G>(a, blockIdx.x, sm);
+        return;
+    }
     if (threadIdx.x == 0) s_tile = atomicAdd(&a.result->tile_ctr, 1u);
     __syncthreads();
     for (;;) {
