@@ -368,19 +368,33 @@ __device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, 
     const uint32_t mult = nf > 1 ? nf : 1u;
     // the child's tuple and anchor row, read once per (member) parent
     my_bytes += (4ull * (d + 1) + 4ull * (re - rs + 1)) * mult;
-    if (a.leaf_count && flags && nf <= 1 && !a.g.elab) {
+    if (a.leaf_count && flags && !a.g.elab) {
         // depth+1 is the last query vertex with nothing to check beyond the
         // anchor edge (no requirement, no row search for the anchor): every
         // entry left in the slice is an embedding -- count them here and
-        // write no child
-        const DLevel *N = &a.plans[q].lv[d + 1];
-        if (N->final_ && N->nreq == 0 && !N->anchor_check) {
-            if (fc && q != fq) {
-                atomicAdd(&a.counts[fq], fc);
-                fc = 0;
+        // write no child.  A branching node whose child nodes all end so
+        // (anchor_check bit 1) counts the slice once for each of them.
+        if (nf <= 1) {
+            const DLevel *N = &a.plans[q].lv[d + 1];
+            if (N->final_ && N->nreq == 0 && !(N->anchor_check & 1u)) {
+                if (fc && q != fq) {
+                    atomicAdd(&a.counts[fq], fc);
+                    fc = 0;
+                }
+                fq = q;
+                fc += len;
+                return false;
             }
-            fq = q;
-            fc += len;
+        } else if (L->anchor_check & 2u) {
+            for (uint32_t j = 0; j < nf; ++j) {
+                const uint32_t qj = __ldg(a.fan_list + L->fan_start + j);
+                if (fc && qj != fq) {
+                    atomicAdd(&a.counts[fq], fc);
+                    fc = 0;
+                }
+                fq = qj;
+                fc += len;
+            }
             return false;
         }
     }
@@ -445,7 +459,7 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
     } else {
         const uint32_t idx = __ldg(a.pcstart + p) + local;
         v = __ldg(a.g.adj + idx);
-        if (L->anchor_check)
+        if (L->anchor_check & 1u)
             pass = has_edge(a.g, __ldg(a.ptup + (uint64_t)(1 + L->anchor) * a.pstride + p), v, L->anchor_lab);
         else if (a.g.elab)
             pass = __ldg(a.g.elab + idx) == L->anchor_lab;
@@ -1538,7 +1552,13 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
                 if (kids.size() > 1) {
                     dq[r].lv[d].fan_count = (uint16_t)kids.size();
                     dq[r].lv[d].fan_start = (uint32_t)fan_list.size();
-                    for (const auto &k : kids) fan_list.push_back(k[0]);
+                    bool leaves = true;  // every child node's depth d+1 is counted at its parent
+                    for (const auto &k : kids) {
+                        fan_list.push_back(k[0]);
+                        const DLevel &N = dq[k[0]].lv[d + 1];
+                        leaves = leaves && N.final_ && N.nreq == 0 && !(N.anchor_check & 1u);
+                    }
+                    if (leaves) dq[r].lv[d].anchor_check |= 2u;
                 }
                 for (auto &k : kids) next.push_back(std::move(k));
             }
@@ -1546,7 +1566,7 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         }
         if (!share) {
             for (DQuery &q : dq)
-                for (DLevel &l : q.lv) l.fan_count = 0, l.fan_start = 0;
+                for (DLevel &l : q.lv) l.fan_count = 0, l.fan_start = 0, l.anchor_check &= 1u;
             fan_list.clear();
             root_rep.clear();
             for (uint32_t i = 0; i < na; ++i) final_rep[i] = i;

@@ -99,7 +99,9 @@ struct alignas(16) DLevel {
     uint8_t nreq;              // extra requirement checks
     uint8_t anchor_lab;        // label of the anchor requirement
     uint8_t final_;            // depth == k-1
-    uint8_t anchor_check;      // anchor requirement needs a row search (multi-edge data)
+    uint8_t anchor_check;      // bit 0: the anchor requirement needs a row search (multi-edge
+                               // data); bit 1 (a branching trie node's representative): every
+                               // child node's depth+1 is a last vertex counted at its parent
     uint16_t next_ub;          // symmetry breaking: depth+1's candidate < tuple[pos] for these positions
     uint8_t req_pos[MAXQ];     // tuple position, or REQ_SELF
     uint8_t req_lab[MAXQ];
