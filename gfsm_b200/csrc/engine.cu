@@ -1389,8 +1389,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     // queries -- runs its whole schedule as one CUDA graph launch (no host
     // round trip per step: plain p50 0.41 -> 0.33 ms on the grid workload);
     // heavier calls run the host-driven loop, whose steps launch one CTA per
-    // tile (the graph's fixed persistent grid runs a step 10-20% slower).  A
-    // single query takes the default geometry, a batch the autotuned one.
+    // tile (the graph's fixed persistent grid runs a large step ~10% slower:
+    // it spills more at the 32-register budget).  A single query takes the
+    // default geometry, a batch the autotuned one.
     const char *drv = getenv("GFSM_DRIVER");
     const bool force_graph = !trace && drv && *drv && !strcmp(drv, "graph");
     const bool force_host = trace || (drv && *drv && strcmp(drv, "graph"));
