@@ -957,6 +957,10 @@ __global__ void __launch_bounds__(G::T, G::MINB) k_step_g() {
     if (threadIdx.x == 0) s_tile = atomicAdd(&a.result->tile_ctr, 1u);
     __syncthreads();
     for (;;) {
+        // (256,4) tiles: values derived from the step's arguments are read
+        // again each tile instead of held across the loop -- that geometry
+        // otherwise spills 88 bytes per thread here, and none with this
+        if constexpr (G::CPT == 4) asm volatile("" ::: "memory");
         const uint32_t tile = s_tile;
         if (tile >= a.ntiles) break;
         uint32_t next = 0;
