@@ -476,7 +476,23 @@ void gfsm_plan_destroy(gfsm_plan *p) { delete p; }
 
 void gfsm_plan_destroy_array(gfsm_plan *const *plans, int n) {
     if (!plans) return;
-    for (int i = 0; i < n; ++i) delete plans[i];
+    // a plan is a dozen small vectors: large batches free on a few host
+    // threads (a worker that cannot be started runs on this thread)
+    const int hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min(hw, n / 256));
+    auto work = [&](int t) {
+        for (int i = t; i < n; i += nt) delete plans[i];
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) {
+        try {
+            pool.emplace_back(work, t);
+        } catch (...) {
+            work(t);
+        }
+    }
+    work(0);
+    for (auto &th : pool) th.join();
 }
 
 gfsm_status gfsm_batch_count(gfsm_ctx *ctx, const gfsm_plan *const *plans, int nq, const gfsm_graph *data,

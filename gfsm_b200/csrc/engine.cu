@@ -1420,8 +1420,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     const bool sym_ok = !rows_out && g.symmetric && !g.multi && g.elab == nullptr && !(symv && *symv == '0');
     const bool vl_on = lim.vertex_labels != 0;
     {
-        // independent per query: large batches use a few host threads
-        std::vector<DQuery> all(nq);
+        // independent per query: large batches use a few host threads; the
+        // plans are built in place and the active ones compacted below
+        dq.resize(nq);
+        std::vector<DQuery> &all = dq;
         std::vector<uint32_t> lo(nq), hi(nq);
         std::vector<char> never(nq, 0);
         std::vector<gfsm_status> qrc(nq, GFSM_OK);
@@ -1438,8 +1440,8 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
         for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
         work(0);
         for (auto &th : pool) th.join();
-        dq.reserve(nq);
         std::vector<uint64_t> cut(nparts + 1);
+        size_t w = 0;
         for (int i = 0; i < nq; ++i) {
             if (qrc[i] != GFSM_OK) return qrc[i];
             if (never[i]) continue;
@@ -1449,12 +1451,14 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
                 lo[i] = base + (uint32_t)cut[part];
                 hi[i] = base + (uint32_t)cut[part + 1];
             }
-            dq.push_back(all[i]);
+            if (w != (size_t)i) all[w] = all[i];
+            ++w;
             active.push_back(i);
             rlo.push_back(lo[i]);
             rhi.push_back(hi[i]);
-            dmax = std::max(dmax, all[i].k - 1);
+            dmax = std::max(dmax, all[w - 1].k - 1);
         }
+        dq.resize(w);
     }
     const uint32_t na = (uint32_t)active.size();
     const auto t_plans = std::chrono::steady_clock::now();
@@ -1565,7 +1569,10 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
                     }
                     if (leaves) dq[r].lv[d].anchor_check |= 2u;
                 }
-                for (auto &k : kids) next.push_back(std::move(k));
+                // a node of one query has no fan-out below it and counts to
+                // itself: it is not carried to deeper levels
+                for (auto &k : kids)
+                    if (k.size() > 1) next.push_back(std::move(k));
             }
             level.swap(next);
         }
