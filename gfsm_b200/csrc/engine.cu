@@ -238,18 +238,25 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
 }
 
 constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
-constexpr int REQ_SMEM = 768;       // entries staged per requirement row
 
 // Tile geometry of a level-step instantiation: threads per CTA, candidates
-// per thread, and the CTAs per SM its register budget is fitted to.
-template <int T_, int CPT_, int MINB_>
+// per thread, the CTAs per SM its register budget is fitted to, and the
+// entries of each requirement row a single-parent tile stages in shared
+// memory.  Shared memory and L1 share one 256 KiB array per SM, and the
+// driver picks the smallest shared-memory carve-out that holds the CTAs the
+// registers allow (196 KiB for 8 CTAs of 21.9 KB), leaving L1 the rest.
+// (256,2) stages only 64 entries per row so that its 8 CTAs fit 132 KiB
+// (124 KiB of L1 instead of 60 KiB: level step 96.1 -> 92.3 ms on the grid
+// batch); longer row parts are searched in global memory over the staged
+// bounds.
+template <int T_, int CPT_, int MINB_, int REQ_ = 768>
 struct Geo {
     static constexpr int T = T_, CPT = CPT_, TILE = T_ * CPT_, WIN = T_ * CPT_ + 2, NWARP = T_ / 32,
-                         WC = 32 * CPT_, MINB = MINB_;
+                         WC = 32 * CPT_, MINB = MINB_, REQ = REQ_;
 };
 using Geo0 = Geo<256, 4, 6>;   // 1024-candidate tiles, 8 warps (the default)
 using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
-using Geo2 = Geo<256, 2, 7>;   // 512-candidate tiles, 8 warps
+using Geo2 = Geo<256, 2, 7, 64>;  // 512-candidate tiles, 8 warps
 using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
 // Survivors one warp stages per tile, at most; their slice counts are
 // summed in 32 bits (see the trie fan-out cap in Engine::run).
@@ -267,7 +274,7 @@ template <class G>
 struct StepSmem {
     unsigned long long coff[G::WIN];
     Stage stage[G::TILE];
-    uint32_t req[NSTAGE][REQ_SMEM];
+    uint32_t req[NSTAGE][G::REQ];
     uint32_t rlo[NSTAGE], rhi[NSTAGE], rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
     uint32_t wcnt[G::NWARP], wofs[G::NWARP + 1];
     unsigned long long wdeg[G::NWARP], wdofs[G::NWARP], wbytes[G::NWARP];
@@ -575,9 +582,9 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
         for (uint32_t r = 0; r < (uint32_t)NSTAGE; ++r) {
             if (r >= L0->nreq || L0->req_pos[r] == REQ_SELF) continue;
             const uint32_t lo = sm.rlo[r], n = sm.rhi[r] - sm.rlo[r];
-            if (n <= (uint32_t)REQ_SMEM)
+            if (n <= (uint32_t)G::REQ)
                 for (uint32_t i = tid; i < n; i += T) sm.req[r][i] = __ldg(a.g.adj + lo + i);
-            if (tid == 0) sm.rmode[r] = n <= (uint32_t)REQ_SMEM ? 1u : 2u;
+            if (tid == 0) sm.rmode[r] = n <= (uint32_t)G::REQ ? 1u : 2u;
         }
     }
     if (tid == 0) sm.q0 = ROOT ? __ldg(a.root_rep + plo) : (__ldg(a.ptup + plo) & kNodeMask);
@@ -586,7 +593,7 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
     uint32_t fq = 0xffffffffu, wcnt = 0;
     Stage *wstage = sm.stage + warp * WC;
-    const CandCtx tctx{win_smem ? sm.coff : nullptr, nwin, plo, single, &sm.req[0][0], (uint32_t)REQ_SMEM,
+    const CandCtx tctx{win_smem ? sm.coff : nullptr, nwin, plo, single, &sm.req[0][0], (uint32_t)G::REQ,
                        sm.rlo, sm.rhi, sm.rmode};
 
 #pragma unroll 1
