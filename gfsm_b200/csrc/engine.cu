@@ -40,6 +40,7 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -240,24 +241,30 @@ __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t *a, uint32_t
 constexpr int NSTAGE = 2;           // requirement rows a single-parent tile stages
 
 // Tile geometry of a level-step instantiation: threads per CTA, candidates
-// per thread, the CTAs per SM its register budget is fitted to, and the
-// entries of each requirement row a single-parent tile stages in shared
-// memory.  Shared memory and L1 share one 256 KiB array per SM, and the
-// driver picks the smallest shared-memory carve-out that holds the CTAs the
-// registers allow (196 KiB for 8 CTAs of 21.9 KB), leaving L1 the rest.
-// (256,2) stages only 64 entries per row so that its 8 CTAs fit 132 KiB
-// (124 KiB of L1 instead of 60 KiB: level step 96.1 -> 92.3 ms on the grid
-// batch); longer row parts are searched in global memory over the staged
-// bounds.
-template <int T_, int CPT_, int MINB_, int REQ_ = 768>
+// per thread, the CTAs per SM its register budget is fitted to, the entries
+// of each requirement row a single-parent tile stages in shared memory, and
+// whether the tile's parent window is kept as 16-bit offsets.  Shared memory
+// and L1 share one 256 KiB array per SM, and the driver picks the smallest
+// shared-memory carve-out that holds the CTAs the registers allow (196 KiB
+// for 8 CTAs of 21.9 KB), leaving L1 the rest -- so shared bytes are L1
+// bytes.  (256,2) stages only 64 entries per row (longer row parts are
+// searched in global memory over the staged bounds): its 8 CTAs fit 132 KiB,
+// 124 KiB of L1 instead of 60 KiB (grid batch level step 96.1 -> 92.3 ms);
+// its 32-register kernel keeps the whole 64-bit window, which measured
+// faster there.  The 40-register geometries take the 16-bit window: (256,4)
+// fits 196 KiB instead of 228 KiB, 60 KiB of L1 instead of 28 KiB (R-MAT
+// triangle 91.1 -> 80.9 ms).
+template <int T_, int CPT_, int MINB_, int REQ_ = 768, bool W16_ = true>
 struct Geo {
     static constexpr int T = T_, CPT = CPT_, TILE = T_ * CPT_, WIN = T_ * CPT_ + 2, NWARP = T_ / 32,
                          WC = 32 * CPT_, MINB = MINB_, REQ = REQ_;
+    static constexpr bool W16 = W16_;
+    using WinT = std::conditional_t<W16_, uint16_t, unsigned long long>;
 };
-using Geo0 = Geo<256, 4, 6>;   // 1024-candidate tiles, 8 warps (the default)
-using Geo1 = Geo<128, 4, 11>;  // 512-candidate tiles, 4 warps
-using Geo2 = Geo<256, 2, 7, 64>;  // 512-candidate tiles, 8 warps
-using Geo3 = Geo<512, 2, 3>;   // 1024-candidate tiles, 16 warps
+using Geo0 = Geo<256, 4, 6>;               // 1024-candidate tiles, 8 warps (the default)
+using Geo1 = Geo<128, 4, 11>;              // 512-candidate tiles, 4 warps
+using Geo2 = Geo<256, 2, 7, 64, false>;    // 512-candidate tiles, 8 warps
+using Geo3 = Geo<512, 2, 3>;               // 1024-candidate tiles, 16 warps
 // Survivors one warp stages per tile, at most; their slice counts are
 // summed in 32 bits (see the trie fan-out cap in Engine::run).
 constexpr uint64_t kWarpStage = 128;
@@ -272,7 +279,14 @@ __host__ __device__ constexpr uint32_t variant_tile(int v) {
 // Shared memory of one tile of a level step.
 template <class G>
 struct StepSmem {
-    unsigned long long coff[G::WIN];
+    static_assert(!G::W16 || G::TILE < 65536, "16-bit window offsets");
+    // the parents' candidate prefix over the tile, win[i] for parent plo+i:
+    // whole (64-bit), or (W16) as the offset from the tile's first candidate
+    // for the parents that start inside the tile (0 < i < nwin-1), with the
+    // first parent's start and the last one's end, which lie outside it,
+    // kept whole in win_ends
+    typename G::WinT win[G::WIN];
+    unsigned long long win_ends[2];
     Stage stage[G::TILE];
     uint32_t req[NSTAGE][G::REQ];
     uint32_t rlo[NSTAGE], rhi[NSTAGE], rmode[NSTAGE];  // mode 0 none, 1 shared, 2 global range
@@ -303,8 +317,10 @@ __device__ __forceinline__ void tile_alloc(const StepArgs &a, const unsigned lon
 // Per-tile context of the candidate check: the parents' candidate prefix
 // window (shared memory, or null to search global memory), and for a tile
 // inside one parent's slice the staged requirement-row slices.
+template <class W>
 struct CandCtx {
-    const unsigned long long *win;
+    const W *win;
+    const unsigned long long *win_ends;
     uint32_t nwin, plo;
     bool single;
     const uint32_t *req;
@@ -411,29 +427,35 @@ __device__ __forceinline__ bool next_slice(const StepArgs &a, const uint32_t d, 
     return true;
 }
 
-// One candidate c of a level step: find its parent, check it (injectivity,
-// anchor label, remaining requirements), and either count it (last query
-// vertex) or describe the child it becomes (emit, rec).
-template <bool ROOT>
+// One candidate c (offset off in its tile) of a level step: find its
+// parent, check it (injectivity, anchor label, remaining requirements), and
+// either count it (last query vertex) or describe the child it becomes
+// (emit, rec).
+template <bool ROOT, class W>
 __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_t d, const unsigned long long c,
-                                                const CandCtx &t, bool &emit, Stage &rec,
+                                                const uint32_t off, const CandCtx<W> &t, bool &emit, Stage &rec,
                                                 unsigned long long &my_bytes, uint32_t &fq, unsigned long long &fc) {
-    // parent = largest p in [plo, phi] with coff[p] <= c
-    uint32_t lo = 0, hi = t.nwin - 1;
-    if (t.win) {
+    constexpr bool W16 = sizeof(W) == 2;
+    // parent = largest p in [plo, phi] with coff[p] <= c; local = c - coff[p]
+    uint32_t lo = 0, hi = t.nwin - 1, local;
+    if (t.win) {  // (W16: the probes only reach parents that start inside the tile)
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (t.win[mid] <= c) lo = mid; else hi = mid;
+            const bool le = W16 ? (uint32_t)t.win[mid] <= off : (unsigned long long)t.win[mid] <= c;
+            if (le) lo = mid; else hi = mid;
         }
+        if constexpr (W16)
+            local = lo == 0 ? (uint32_t)(c - t.win_ends[0]) : off - (uint32_t)t.win[lo];
+        else
+            local = (uint32_t)(c - t.win[lo]);
     } else {
         while (hi - lo > 1) {
             const uint32_t mid = lo + ((hi - lo) >> 1);
             if (__ldg(a.pcoff + t.plo + mid) <= c) lo = mid; else hi = mid;
         }
+        local = (uint32_t)(c - __ldg(a.pcoff + t.plo + lo));
     }
     const uint32_t p = t.plo + lo;
-    const unsigned long long pc = t.win ? t.win[lo] : __ldg(a.pcoff + p);
-    uint32_t local = (uint32_t)(c - pc);
     uint32_t q = ROOT ? __ldg(a.root_rep + p) : __ldg(a.ptup + p);
     const uint32_t excl = ROOT ? 0u : (q >> kExclShift) & 0xffu;
     const bool inj_done = !ROOT && (q & kInjDone);
@@ -442,8 +464,16 @@ __device__ __forceinline__ void check_candidate(const StepArgs &a, const uint32_
         // node, row offset), one copy of its slice per child node
         q &= kNodeMask;
         const DLevel *P = &a.plans[q].lv[d - 1];
-        const unsigned long long pn = t.win ? t.win[lo + 1] : __ldg(a.pcoff + p + 1);
-        const uint32_t slen = (uint32_t)(pn - pc) / P->fan_count;  // the fan-out cap keeps pn - pc < 2^32
+        // the parent's candidates: local + (its end - c), below 2^32 by the
+        // fan-out cap
+        uint32_t span;
+        if (!t.win)
+            span = local + (uint32_t)(__ldg(a.pcoff + p + 1) - c);
+        else if constexpr (W16)
+            span = local + (lo + 2 == t.nwin ? (uint32_t)(t.win_ends[1] - c) : (uint32_t)t.win[lo + 1] - off);
+        else
+            span = (uint32_t)(t.win[lo + 1] - t.win[lo]);
+        const uint32_t slen = span / P->fan_count;
         const uint32_t j = local / slen;
         local -= j * slen;
         q = __ldg(a.fan_list + P->fan_start + j);
@@ -548,7 +578,16 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     const uint32_t nwin = phi - plo + 2;  // coff[plo .. phi+1]
     const bool win_smem = nwin <= (uint32_t)WIN;
     if (win_smem)
-        for (uint32_t i = tid; i < nwin; i += T) sm.coff[i] = __ldg(a.pcoff + plo + i);
+        for (uint32_t i = tid; i < nwin; i += T) {
+            const unsigned long long x = __ldg(a.pcoff + plo + i);
+            if constexpr (G::W16) {
+                if (i == 0) sm.win_ends[0] = x;
+                if (i == nwin - 1) sm.win_ends[1] = x;
+                sm.win[i] = (i == 0 || i == nwin - 1) ? (uint16_t)0 : (uint16_t)(x - base);
+            } else {
+                sm.win[i] = x;
+            }
+        }
     const uint32_t d = a.depth;
     const bool emits = a.ctup != nullptr;
 
@@ -593,15 +632,16 @@ __device__ __forceinline__ void step_tile(const StepArgs &a, const uint32_t tile
     unsigned long long my_bytes = 0, fc = 0, my_deg = 0;
     uint32_t fq = 0xffffffffu, wcnt = 0;
     Stage *wstage = sm.stage + warp * WC;
-    const CandCtx tctx{win_smem ? sm.coff : nullptr, nwin, plo, single, &sm.req[0][0], (uint32_t)G::REQ,
+    const CandCtx<typename G::WinT> tctx{win_smem ? sm.win : nullptr, sm.win_ends, nwin, plo, single, &sm.req[0][0], (uint32_t)G::REQ,
                        sm.rlo, sm.rhi, sm.rmode};
 
 #pragma unroll 1
     for (int j = 0; j < CPT; ++j) {
-        const unsigned long long c = base + (unsigned long long)(warp * WC + j * 32) + lane;
+        const uint32_t off = warp * WC + j * 32 + lane;
+        const unsigned long long c = base + off;
         bool emit = false;
         Stage rec{0, 0, 0, 0, 0};
-        if (c < tend) check_candidate<ROOT>(a, d, c, tctx, emit, rec, my_bytes, fq, fc);
+        if (c < tend) check_candidate<ROOT>(a, d, c, off, tctx, emit, rec, my_bytes, fq, fc);
         if (emits) {
             const uint32_t bal = __ballot_sync(0xffffffffu, emit);
             if (emit) wstage[wcnt + __popc(bal & ((1u << lane) - 1u))] = rec;
@@ -1353,28 +1393,51 @@ int Engine::pick_variant(const std::vector<const Plan *> &plans, const DeviceGra
             }
         return best;
     }
+    // The samples run on the driver the whole call takes -- the graph for a
+    // light call (first level of at most kGraphRootEntries candidates), else
+    // the host loop -- since a geometry's graph kernel and its one-CTA-per-
+    // tile kernel rank differently (the grid batch: (256,2) did not beat
+    // (256,4) by 2% on a 128-query sample on the graph, and takes the whole
+    // batch 7% faster on the host loop).  Geometries are compared on
+    // level-step time, which the host loop's round trips do not dilute.
+    uint64_t first_level = 0;
+    for (size_t i = 0; i < plans.size() && first_level <= kGraphRootEntries; ++i) {
+        DQuery dq;
+        uint32_t lo = 0, hi = 0;
+        bool never = false;
+        if (build_dquery(*plans[i], g, lim, dq, lo, hi, never) == GFSM_OK && !never)
+            first_level += (uint64_t)g.h_rowptr[hi] - g.h_rowptr[lo];
+    }
+    const bool heavy = first_level > kGraphRootEntries;
+    struct DriverScope {
+        int &d;
+        ~DriverScope() { d = -1; }
+    } scope{tune_driver};
+    tune_driver = heavy ? 0 : 1;
     // The sample is the call's first 32 queries, grown fourfold (up to 2,048)
-    // while the default geometry takes under 2 ms on it: shorter samples are
-    // launch-bound and their timings mostly noise.  Another geometry must
-    // beat the default by 2% to be chosen (repeat timings of a sample agree
-    // within ~0.5%).
+    // while the default geometry takes under 2 ms on it (8 ms for a host-loop
+    // call, whose steps at full size are many waves long): shorter samples
+    // are launch-bound and their timings mostly noise.  Another geometry
+    // must beat the default by 2% to be chosen (repeat timings of a sample
+    // agree within ~0.5%).
+    const double min_ms = heavy ? 8.0 : 2.0;
     int best = 0;
     for (size_t ns = std::min<size_t>(plans.size(), 32);; ns = std::min<size_t>(plans.size(), ns * 4)) {
         std::vector<const Plan *> sample(plans.begin(), plans.begin() + ns);
         std::vector<uint64_t> cnt(ns);
         gfsm_stats s0{};
         if (run(sample, g, lim, cnt.data(), &s0, nullptr, 0, nullptr, err, 0) != GFSM_OK) return 0;
-        const double base_ms = s0.device_ms;
-        if (base_ms < 2.0) {
+        if (s0.device_ms < min_ms) {
             if (ns < plans.size() && ns < 2048) continue;
             break;  // the whole call is short: keep the default
         }
+        const double base_ms = s0.kernel_ms;
         double best_ms = base_ms;
         for (int v = 1; v < kVariants; ++v) {
             gfsm_stats sv{};
             if (run(sample, g, lim, cnt.data(), &sv, nullptr, 0, nullptr, err, v) != GFSM_OK) return 0;
-            if (sv.device_ms < best_ms && sv.device_ms < 0.98 * base_ms) {
-                best_ms = sv.device_ms;
+            if (sv.kernel_ms < best_ms && sv.kernel_ms < 0.98 * base_ms) {
+                best_ms = sv.kernel_ms;
                 best = v;
             }
         }
@@ -1404,8 +1467,9 @@ gfsm_status Engine::run(const std::vector<const Plan *> &plans, const DeviceGrap
     // it spills more at the 32-register budget).  A single query takes the
     // default geometry, a batch the autotuned one.
     const char *drv = getenv("GFSM_DRIVER");
-    const bool force_graph = !trace && drv && *drv && !strcmp(drv, "graph");
-    const bool force_host = trace || (drv && *drv && strcmp(drv, "graph"));
+    const bool env_drv = drv && *drv;
+    const bool force_graph = !trace && ((env_drv && !strcmp(drv, "graph")) || (!env_drv && tune_driver == 1));
+    const bool force_host = trace || (env_drv && strcmp(drv, "graph")) || (!env_drv && tune_driver == 0);
     if (variant < 0) variant = (plans.size() <= 1) ? 0 : pick_variant(plans, g, lim, err);
     auto t_start = std::chrono::steady_clock::now();
     const int nq = (int)plans.size();

@@ -64,6 +64,9 @@ struct Engine {
     // instead of the conservative first-step cap
     std::map<uint64_t, std::vector<double>> nxt_seen;
     bool autotune = true;           // off for served slots: tuning runs would sit on the request path
+    // the driver tuning runs take (that of the call being tuned): 0 host
+    // loop, 1 graph; -1 outside tuning (chosen by the call's size)
+    int tune_driver = -1;
 };
 
 }  // namespace gfsm
