@@ -9,7 +9,6 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
-#include <functional>
 #include <thread>
 
 #include "gfsm_internal.h"
@@ -184,42 +183,67 @@ gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGra
 // ---------------------------------------------------------------------------
 // Planner
 // ---------------------------------------------------------------------------
+// Stable insertion sort of a short range by key (query rows and requirement
+// lists hold a few entries; the reference orders them with stable sorts).
+template <class T, class Key>
+static void stable_small_sort(T *b, T *e, Key key) {
+    if (e - b > 32) {
+        std::stable_sort(b, e, [&](const T &x, const T &y) { return key(x) < key(y); });
+        return;
+    }
+    for (T *i = b + 1; i < e; ++i) {
+        const T x = *i;
+        T *j = i;
+        for (; j > b && key(*(j - 1)) > key(x); --j) *j = *(j - 1);
+        *j = x;
+    }
+}
+
 gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std::vector<double> *weight) {
     p = Plan();
     p.rel_bits = rel_bits;
     const uint32_t k = q.n;
     if (k == 0) return GFSM_ERR_QUERY;
     if (k > (uint32_t)MAXQ) return GFSM_ERR_TOO_LARGE;
-    std::vector<uint32_t> deg(k, 0);
-    for (uint32_t s : q.src) deg[s]++;
+    const size_t m = q.src.size();
+    uint32_t deg[MAXQ] = {};
+    for (uint32_t s : q.src) {
+        if (s >= k) return GFSM_ERR_QUERY;
+        deg[s]++;
+    }
+    for (uint32_t d : q.dst)
+        if (d >= k) return GFSM_ERR_QUERY;
     for (uint32_t v = 0; v < k; ++v)
         if (!deg[v]) return GFSM_ERR_QUERY;  // no row: the reference walks past its CCSR
     // Query CCSR rows: degree descending, id ascending (HnHelper.cuh:26-31).
-    std::vector<uint32_t> rowvid(k), rowidx(k);
+    uint32_t rowvid[MAXQ], rowidx[MAXQ];
     for (uint32_t v = 0; v < k; ++v) rowvid[v] = v;
-    std::stable_sort(rowvid.begin(), rowvid.end(),
-                     [&](uint32_t a, uint32_t b) { return deg[a] > deg[b]; });
+    stable_small_sort(rowvid, rowvid + k, [&](uint32_t v) { return -(int64_t)deg[v]; });
     for (uint32_t i = 0; i < k; ++i) rowidx[rowvid[i]] = i;
-    // rows[i] = (target row, label) sorted by target (HnHelper.cuh:470-478)
-    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> rows(k);
-    for (size_t e = 0; e < q.src.size(); ++e)
-        rows[rowidx[q.src[e]]].push_back({rowidx[q.dst[e]], q.lab[e]});
+    // row i = ent[rs[i], rs[i+1]): (target row, label) sorted by target
+    // (HnHelper.cuh:470-478), entries of equal target in input order
+    using Ent = std::pair<uint32_t, uint32_t>;
+    uint32_t rs[MAXQ + 1] = {}, fill[MAXQ];
+    for (uint32_t v = 0; v < k; ++v) rs[rowidx[v] + 1] = deg[v];
+    for (uint32_t i = 0; i < k; ++i) rs[i + 1] += rs[i];
+    std::copy(rs, rs + k, fill);
+    std::vector<Ent> ent(m);
+    for (size_t e = 0; e < m; ++e) ent[fill[rowidx[q.src[e]]]++] = {rowidx[q.dst[e]], q.lab[e]};
     uint32_t maxv = 0;
-    for (auto &r : rows) {
-        std::stable_sort(r.begin(), r.end(),
-                         [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
-                             return a.first < b.first;
-                         });
-        maxv = std::max<uint32_t>(maxv, (uint32_t)r.size());
+    for (uint32_t i = 0; i < k; ++i) {
+        stable_small_sort(ent.data() + rs[i], ent.data() + rs[i + 1], [](const Ent &x) { return x.first; });
+        maxv = std::max(maxv, rs[i + 1] - rs[i]);
     }
+    const Ent *E = ent.data();
     p.k = k;
     p.max_valency = maxv;
     p.order.assign(k, 0);
     p.header.assign(3 * (size_t)k, 0);
     p.reqs.assign(2 * (size_t)maxv * k, 0);
-    std::vector<int32_t> mapping(k, -1);
     // mapping[r]: -1 unseen, 0 seen (a neighbour of a placed row), d + 1 for
     // a row placed d depths ago.
+    int32_t mapping[MAXQ];
+    std::fill(mapping, mapping + k, -1);
     if (!weight) {
         mapping[0] = 0;  // HnGPU.cu:759-769: the first row has the maximal degree
     } else {
@@ -227,11 +251,13 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
         uint32_t best = 0;
         double best_c = 0.0;
         for (uint32_t r = 0; r < k; ++r) {
-            const double c = (*weight)[rowvid[r]] / (double)rows[r].size();
+            const double c = (*weight)[rowvid[r]] / (double)(rs[r + 1] - rs[r]);
             if (r == 0 || c < best_c) { best = r; best_c = c; }
         }
         mapping[best] = 0;
     }
+    std::vector<Ent> rr;
+    rr.reserve(maxv);
     for (uint32_t depth = 0; depth < k; ++depth) {  // HnGPU.cu:771-773
         uint32_t rel_depth = 0;
         bool found = false;
@@ -254,10 +280,10 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
             for (uint32_t i = 0; i < k; ++i) {
                 if (mapping[i] != 0) continue;
                 uint32_t back = 0, last = ~0u;
-                for (auto &ent : rows[i])
-                    if (ent.first != last) {
-                        last = ent.first;
-                        back += mapping[ent.first] > 0 ? 1u : 0u;
+                for (uint32_t x = rs[i]; x < rs[i + 1]; ++x)
+                    if (E[x].first != last) {
+                        last = E[x].first;
+                        back += mapping[last] > 0 ? 1u : 0u;
                     }
                 const double c = (*weight)[rowvid[i]];
                 if (!found || back > best_back || (back == best_back && c < best_c)) {
@@ -276,24 +302,21 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
         if (!found) return GFSM_ERR_QUERY;  // ccsr.cpp:126-128
         p.order[depth] = rel_depth;
         // ccsr.cpp:142-167
-        std::vector<std::pair<uint32_t, uint32_t>> rr;
-        for (auto &ent : rows[rel_depth]) {
-            uint32_t t = ent.first;
+        rr.clear();
+        for (uint32_t x = rs[rel_depth]; x < rs[rel_depth + 1]; ++x) {
+            const uint32_t t = E[x].first;
             if (mapping[t] < 0) mapping[t] = 0;
             if (mapping[t] > 0) {
-                uint32_t rel = ent.second;
-                for (auto &back : rows[t])
-                    if (back.first == rel_depth) { rel = back.second; break; }
+                uint32_t rel = E[x].second;
+                for (uint32_t y = rs[t]; y < rs[t + 1]; ++y)
+                    if (E[y].first == rel_depth) { rel = E[y].second; break; }
                 rr.push_back({(uint32_t)(mapping[t] - 1), rel});
             }
         }
         // ccsr.cpp:169-196
         uint32_t firstq = 0, off = depth * maxv * 2;
         if (!rr.empty()) {
-            std::stable_sort(rr.begin(), rr.end(),
-                             [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
-                                 return a.first < b.first;
-                             });
+            stable_small_sort(rr.data(), rr.data() + rr.size(), [](const Ent &x) { return x.first; });
             p.reqs[off] = rr[0].first;
             p.reqs[off + 1] = rr[0].second;
             for (size_t i = 1; i < rr.size(); ++i) {
@@ -319,35 +342,32 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
     p.qlabel.resize(k);
     p.qdeg.resize(k);
     for (uint32_t d = 0; d < k; ++d) {
-        uint32_t v = rowvid[p.order[d]];
+        const uint32_t r = p.order[d], v = rowvid[r];
         p.qvid[d] = v;
         p.qlabel[d] = v < q.vlabel.size() ? q.vlabel[v] : 0;
-        std::vector<uint32_t> nb;
-        for (auto &ent : rows[p.order[d]])
-            if (ent.first != p.order[d]) nb.push_back(ent.first);
-        std::sort(nb.begin(), nb.end());
-        p.qdeg[d] = (uint32_t)(std::unique(nb.begin(), nb.end()) - nb.begin());
+        uint32_t nb = 0;  // distinct neighbour rows other than itself (k <= 32)
+        for (uint32_t x = rs[r]; x < rs[r + 1]; ++x)
+            if (E[x].first != r) nb |= 1u << E[x].first;
+        p.qdeg[d] = (uint32_t)__builtin_popcount(nb);
     }
+    // does row t hold (u, label)?  (any label when label < 0)
+    auto holds = [&](uint32_t t, uint32_t u, int64_t label) {
+        for (uint32_t y = rs[t]; y < rs[t + 1]; ++y)
+            if (E[y].first == u && (label < 0 || E[y].second == (uint32_t)label)) return true;
+        return false;
+    };
     bool sym = true;
     for (uint32_t u = 0; u < k && sym; ++u)
-        for (auto &ent : rows[u]) {
-            bool back = false;
-            for (auto &b : rows[ent.first])
-                if (b.first == u) { back = true; break; }
-            if (!back) { sym = false; break; }
-        }
+        for (uint32_t x = rs[u]; x < rs[u + 1]; ++x)
+            if (!holds(E[x].first, u, -1)) { sym = false; break; }
     p.symmetric = sym;
     // every entry has its reverse with the same label, and no (row, target)
     // pair repeats: a count that cannot depend on the matching order
     bool inv = sym;
     for (uint32_t u = 0; u < k && inv; ++u)
-        for (size_t i = 0; i < rows[u].size() && inv; ++i) {
-            const auto &ent = rows[u][i];
-            if (i && rows[u][i - 1].first == ent.first) { inv = false; break; }
-            bool back = false;
-            for (auto &b : rows[ent.first])
-                if (b.first == u && b.second == ent.second) { back = true; break; }
-            inv = back;
+        for (uint32_t x = rs[u]; x < rs[u + 1] && inv; ++x) {
+            if (x > rs[u] && E[x - 1].first == E[x].first) { inv = false; break; }
+            inv = holds(E[x].first, u, E[x].second);
         }
     p.order_invariant = inv;
     p.planner = weight ? 1 : 0;
@@ -369,22 +389,22 @@ void plan_symmetry(const HostGraph &q, Plan &p, bool vl) {
     if (!p.order_invariant || k < 2 || k > (uint32_t)MAXQ || p.qvid.size() != k) return;
     // edge label of each ordered pair (0: no edge; labels are >= 1 here or
     // the pair is absent), self-loops on the diagonal
-    std::vector<uint32_t> lab((size_t)k * k, 0);
+    uint32_t lab[MAXQ * MAXQ] = {};
     for (size_t e = 0; e < q.src.size(); ++e) lab[(size_t)q.src[e] * k + q.dst[e]] = (uint32_t)q.lab[e] + 1u;
-    std::vector<uint32_t> deg(k, 0);
-    for (uint32_t a = 0; a < k; ++a)
+    uint32_t deg[MAXQ] = {}, vlab[MAXQ] = {};
+    for (uint32_t a = 0; a < k; ++a) {
         for (uint32_t b = 0; b < k; ++b) deg[a] += lab[(size_t)a * k + b] != 0;
+        vlab[a] = vl && a < q.vlabel.size() ? q.vlabel[a] : 0;
+    }
     auto same_kind = [&](uint32_t a, uint32_t b) {
-        if (deg[a] != deg[b] || lab[(size_t)a * k + a] != lab[(size_t)b * k + b]) return false;
-        return !vl || (a < q.vlabel.size() ? q.vlabel[a] : 0) == (b < q.vlabel.size() ? q.vlabel[b] : 0);
+        return deg[a] == deg[b] && lab[(size_t)a * k + a] == lab[(size_t)b * k + b] && vlab[a] == vlab[b];
     };
     uint64_t budget = 1u << 22;  // search nodes over the whole analysis
-    std::vector<int32_t> img(k), pre(k);
-    // is there an automorphism fixing base[0..nb) with a -> w?
-    std::function<bool(const std::vector<uint32_t> &, uint32_t)> extend;
-    std::vector<uint32_t> todo;
-    extend = [&](const std::vector<uint32_t> &seq, uint32_t i) -> bool {
-        if (i == seq.size()) return true;
+    int32_t img[MAXQ], pre[MAXQ];
+    uint32_t seq[MAXQ], nseq = 0;
+    // extend the partial automorphism img along seq[i..nseq)
+    auto extend = [&](auto &&self, uint32_t i) -> bool {
+        if (i == nseq) return true;
         if (budget == 0) return false;
         --budget;
         const uint32_t a = seq[i];
@@ -398,45 +418,50 @@ void plan_symmetry(const HostGraph &q, Plan &p, bool vl) {
             if (!ok) continue;
             img[a] = (int32_t)w;
             pre[w] = (int32_t)a;
-            if (extend(seq, i + 1)) return true;
+            if (self(self, i + 1)) return true;
             img[a] = -1;
             pre[w] = -1;
         }
         return false;
     };
-    auto exists = [&](const std::vector<uint32_t> &fixed, uint32_t a, uint32_t w) {
-        std::fill(img.begin(), img.end(), -1);
-        std::fill(pre.begin(), pre.end(), -1);
-        for (uint32_t x : fixed) img[x] = (int32_t)x, pre[x] = (int32_t)x;
+    uint32_t fixed[MAXQ], nfixed = 0, fixed_mask = 0;
+    // is there an automorphism fixing fixed[0..nfixed) with a -> w?
+    auto exists = [&](uint32_t a, uint32_t w) {
+        std::fill(img, img + k, -1);
+        std::fill(pre, pre + k, -1);
+        for (uint32_t i = 0; i < nfixed; ++i) img[fixed[i]] = pre[fixed[i]] = (int32_t)fixed[i];
         if (pre[w] >= 0 || !same_kind(a, w)) return false;
-        for (uint32_t x : fixed)
+        for (uint32_t i = 0; i < nfixed; ++i) {
+            const uint32_t x = fixed[i];
             if (lab[(size_t)a * k + x] != lab[(size_t)w * k + x] || lab[(size_t)x * k + a] != lab[(size_t)x * k + w])
                 return false;
+        }
         img[a] = (int32_t)w;
         pre[w] = (int32_t)a;
         // the rest in matching order (neighbours of placed vertices first)
-        std::vector<uint32_t> seq(fixed);
-        seq.push_back(a);
+        nseq = 0;
+        for (uint32_t i = 0; i < nfixed; ++i) seq[nseq++] = fixed[i];
+        seq[nseq++] = a;
         for (uint32_t d = 0; d < k; ++d)
-            if (img[p.qvid[d]] < 0) seq.push_back(p.qvid[d]);
-        return extend(seq, (uint32_t)fixed.size() + 1);
+            if (img[p.qvid[d]] < 0) seq[nseq++] = p.qvid[d];
+        return extend(extend, nfixed + 1);
     };
-    std::vector<uint32_t> fixed;
     uint64_t aut = 1;
     std::vector<std::pair<uint32_t, uint32_t>> cond;
     for (uint32_t d = 0; d < k; ++d) {
         const uint32_t b = p.qvid[d];
         uint64_t orbit = 1;
         for (uint32_t w = 0; w < k; ++w) {
-            if (w == b || std::find(fixed.begin(), fixed.end(), w) != fixed.end()) continue;
-            if (exists(fixed, b, w)) {
+            if (w == b || (fixed_mask >> w & 1u)) continue;
+            if (exists(b, w)) {
                 ++orbit;
                 cond.push_back({b, w});
             }
             if (budget == 0) return;  // too large to analyse: no symmetry breaking
         }
         aut *= orbit;
-        fixed.push_back(b);
+        fixed[nfixed++] = b;
+        fixed_mask |= 1u << b;
     }
     p.aut = aut;
     p.sym_cond = std::move(cond);
