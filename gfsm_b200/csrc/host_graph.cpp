@@ -183,22 +183,6 @@ gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGra
 // ---------------------------------------------------------------------------
 // Planner
 // ---------------------------------------------------------------------------
-// Stable insertion sort of a short range by key (query rows and requirement
-// lists hold a few entries; the reference orders them with stable sorts).
-template <class T, class Key>
-static void stable_small_sort(T *b, T *e, Key key) {
-    if (e - b > 32) {
-        std::stable_sort(b, e, [&](const T &x, const T &y) { return key(x) < key(y); });
-        return;
-    }
-    for (T *i = b + 1; i < e; ++i) {
-        const T x = *i;
-        T *j = i;
-        for (; j > b && key(*(j - 1)) > key(x); --j) *j = *(j - 1);
-        *j = x;
-    }
-}
-
 gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std::vector<double> *weight) {
     p = Plan();
     p.rel_bits = rel_bits;
@@ -218,10 +202,13 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
     // Query CCSR rows: degree descending, id ascending (HnHelper.cuh:26-31).
     uint32_t rowvid[MAXQ], rowidx[MAXQ];
     for (uint32_t v = 0; v < k; ++v) rowvid[v] = v;
-    stable_small_sort(rowvid, rowvid + k, [&](uint32_t v) { return -(int64_t)deg[v]; });
+    std::sort(rowvid, rowvid + k, [&](uint32_t a, uint32_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
     for (uint32_t i = 0; i < k; ++i) rowidx[rowvid[i]] = i;
-    // row i = ent[rs[i], rs[i+1]): (target row, label) sorted by target
-    // (HnHelper.cuh:470-478), entries of equal target in input order
+    // row i = ent[rs[i], rs[i+1]): (target row, label) in input order, then
+    // -- only if not in target order already -- sorted by target alone with
+    // std::sort, the reference's steps (HnHelper.cuh:469-478): the order it
+    // leaves entries of equal target in (their labels pick a requirement's
+    // relation below) is the reference's own
     using Ent = std::pair<uint32_t, uint32_t>;
     uint32_t rs[MAXQ + 1] = {}, fill[MAXQ];
     for (uint32_t v = 0; v < k; ++v) rs[rowidx[v] + 1] = deg[v];
@@ -230,8 +217,10 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
     std::vector<Ent> ent(m);
     for (size_t e = 0; e < m; ++e) ent[fill[rowidx[q.src[e]]]++] = {rowidx[q.dst[e]], q.lab[e]};
     uint32_t maxv = 0;
+    auto by_target = [](const Ent &x, const Ent &y) { return x.first < y.first; };
     for (uint32_t i = 0; i < k; ++i) {
-        stable_small_sort(ent.data() + rs[i], ent.data() + rs[i + 1], [](const Ent &x) { return x.first; });
+        Ent *b = ent.data() + rs[i], *e = ent.data() + rs[i + 1];
+        if (!std::is_sorted(b, e, by_target)) std::sort(b, e, by_target);
         maxv = std::max(maxv, rs[i + 1] - rs[i]);
     }
     const Ent *E = ent.data();
@@ -316,7 +305,7 @@ gfsm_status plan_query(const HostGraph &q, uint32_t rel_bits, Plan &p, const std
         // ccsr.cpp:169-196
         uint32_t firstq = 0, off = depth * maxv * 2;
         if (!rr.empty()) {
-            stable_small_sort(rr.data(), rr.data() + rr.size(), [](const Ent &x) { return x.first; });
+            std::sort(rr.begin(), rr.end(), by_target);  // by distance alone (ccsr.cpp:82-84, 170)
             p.reqs[off] = rr[0].first;
             p.reqs[off + 1] = rr[0].second;
             for (size_t i = 1; i < rr.size(); ++i) {

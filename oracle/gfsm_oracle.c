@@ -71,12 +71,18 @@ static int ord_cmp(const void *a, const void *b)
     return x->id < y->id ? -1 : (x->id > y->id);
 }
 
-typedef struct { uint32_t val, lab; } seg_pair;
+/* A row's entries by target alone, entries of equal target in their input
+ * order (pos): what the reference's std::sort with nodeCompare
+ * (ccsr.cpp:13-16) leaves them in for rows of up to 16 entries (libstdc++
+ * insertion-sorts such ranges) and for rows already in target order, which
+ * it does not sort (HnHelper.cuh:469-478).  A longer unsorted row with a
+ * repeated target may come out of std::sort in another tie order. */
+typedef struct { uint32_t val, lab, pos; } seg_pair;
 static int seg_cmp(const void *a, const void *b)
 {
     const seg_pair *x = a, *y = b;
     if (x->val != y->val) return x->val < y->val ? -1 : 1;
-    return x->lab < y->lab ? -1 : (x->lab > y->lab);
+    return x->pos < y->pos ? -1 : (x->pos > y->pos);
 }
 
 void orc_graph_free(orc_graph *g)
@@ -199,7 +205,7 @@ int orc_parse_buffer(const char *buf, uint64_t len, uint32_t rel_bits, orc_graph
     seg_pair *tmp = malloc(sizeof(seg_pair) * (maxlen ? maxlen : 1));
     for (uint64_t i = 0; i < alloc;) {
         uint32_t sz = g->seg_val[i];
-        for (uint32_t j = 0; j < sz; j++) { tmp[j].val = g->seg_val[i + 1 + j]; tmp[j].lab = g->seg_lab[i + 1 + j]; }
+        for (uint32_t j = 0; j < sz; j++) { tmp[j].val = g->seg_val[i + 1 + j]; tmp[j].lab = g->seg_lab[i + 1 + j]; tmp[j].pos = j; }
         qsort(tmp, sz, sizeof(seg_pair), seg_cmp);
         for (uint32_t j = 0; j < sz; j++) { g->seg_val[i + 1 + j] = tmp[j].val; g->seg_lab[i + 1 + j] = tmp[j].lab; }
         i += sz + 1;
@@ -240,11 +246,14 @@ void orc_pack_segments(const orc_graph *g, uint32_t rel_bits, uint32_t *out)
 /* 2. Planner (HnGPU.cu:749-816, ccsr.cpp:98-219)                            */
 /* ------------------------------------------------------------------------- */
 
-typedef struct { uint32_t req, rel; } req_rel;
+/* Requirements by distance alone (ccsr.cpp:82-84, 170), equal distances in
+ * the order they were found (pos), as std::sort leaves up to 16 of them. */
+typedef struct { uint32_t req, rel, pos; } req_rel;
 static int req_cmp(const void *a, const void *b)
 {
     const req_rel *x = a, *y = b;
-    return x->req < y->req ? -1 : (x->req > y->req);
+    if (x->req != y->req) return x->req < y->req ? -1 : 1;
+    return x->pos < y->pos ? -1 : (x->pos > y->pos);
 }
 
 static uint32_t max_valency(const orc_graph *g) /* ccsr.cpp:206-219 */
@@ -293,6 +302,7 @@ static int gen_reqs(const orc_graph *q, const uint32_t *rowoff, uint32_t maxv, u
             }
             rr[nreq].req = (uint32_t)(mapping[idx] - 1);
             rr[nreq].rel = vert_bits >= 32 ? 0u : rel << vert_bits; /* relation bits, as packed */
+            rr[nreq].pos = nreq;
             nreq++;
         }
     }

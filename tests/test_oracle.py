@@ -183,6 +183,57 @@ def test_reference_frontend_live(tmp_path):
         assert r["reqs"].tolist() == REF["queries/" + name]["reqs"]
 
 
+@pytest.mark.skipif(not os.path.exists(O.REF_FRONTEND), reason="reference front-end not built here")
+def test_reference_frontend_live_irregular_queries(tmp_path):
+    """The reference's own planner on queries with repeated edges (one pair
+    under two labels), self-loops, one-way edges and three edge labels: where
+    it plans the query, the product's planner and the oracle give its
+    requirement table bit for bit; where it exits, both reject the query.
+    Every vertex has a row (the reference walks past its CCSR otherwise) and
+    no row holds more than 16 entries."""
+    import gfsm_b200
+    ctx = gfsm_b200.GFSM(device=-1)
+    rng = np.random.default_rng(23)
+    planned = rejected = 0
+    for i in range(120):
+        k = int(rng.integers(2, 13))
+        edges = []
+        for v in range(1, k):
+            u, l = int(rng.integers(v)), int(rng.integers(1, 4))
+            edges.append((u, v, l))
+            edges.append((v, u, l if rng.random() < 0.8 else int(rng.integers(1, 4))))
+        for _ in range(int(rng.integers(0, k + 1))):
+            a, b, l = int(rng.integers(k)), int(rng.integers(k)), int(rng.integers(1, 4))
+            edges.append((a, b, l))
+            if rng.random() < 0.6:
+                edges.append((b, a, l))
+        rng.shuffle(edges)
+        out = np.bincount(np.array([a for a, _, _ in edges], np.int64), minlength=k)
+        if out.min() == 0 or out.max() > 16:
+            continue
+        lines = ["t # 0", f"{k} {len(edges)} 1 1"] + [f"v {v} 1" for v in range(k)]
+        lines += [f"e {a} {b} {l}" for a, b, l in edges] + ["t # -1"]
+        path = tmp_path / f"q{i}.g"
+        path.write_text("\n".join(lines) + "\n")
+        rc, r = O.ref_frontend_dump(str(path), plan=True)
+        orc = O.Plan(O.Graph(path=str(path)))
+        try:
+            mine = ctx.pre_process_query(ctx.file_parse(str(path))).tables()
+        except gfsm_b200.GFSMError:
+            mine = None
+        if rc != 0:
+            assert mine is None and orc.err, (i, rc, edges)
+            rejected += 1
+            continue
+        assert mine is not None and not orc.err, (i, edges)
+        t = orc.tables()
+        assert t["reqs"].tolist() == r["reqs"].tolist() and t["header"].tolist() == r["header"].tolist(), (i, edges)
+        assert mine["reqs"].tolist() == r["reqs"].tolist() and mine["header"].tolist() == r["header"].tolist(), (i, edges)
+        planned += 1
+    ctx.close()
+    assert planned > 40
+
+
 @pytest.mark.parametrize("vl", [False, True])
 def test_data_aware_order_counts_the_same(tmp_path, vl):
     """Plans from gfsm_query_prepare_for (data-aware matching order), run by
