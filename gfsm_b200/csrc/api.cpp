@@ -180,8 +180,8 @@ gfsm_status gfsm_graph_load_buffer(gfsm_ctx *ctx, const char *buf, uint64_t len,
 gfsm_status gfsm_graph_load_text(gfsm_ctx *ctx, const char *path, gfsm_graph **out) {
     if (!ctx || !path || !out) return GFSM_ERR_ARG;
     *out = nullptr;
-    std::string text;
-    gfsm_status rc = read_file(path, text);
+    FileBytes text;
+    gfsm_status rc = text.open(path);
     if (rc != GFSM_OK) return set_err(ctx, rc, std::string("missing file ") + path);
     return gfsm_graph_load_buffer(ctx, text.data(), text.size(), out);
 }

@@ -4,6 +4,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gfsm.h"
@@ -20,13 +21,38 @@ constexpr uint64_t kMaxScanSize = 500'000'000ull;
 constexpr uint64_t kMemLimit = 22'000'000'000ull;
 constexpr uint64_t kUpperMemLimit = 44'000'000'000ull;
 
+// Allocator whose resize() leaves new elements uninitialised: the code that
+// resizes the edge arrays below writes every element, on several threads,
+// which then also take the first-touch page faults instead of one thread
+// zeroing tens of MB first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <class U>
+    void construct(U *p) noexcept {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a) {
+        ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using RawVec = std::vector<T, NoInitAlloc<T>>;
+
 // ---------------------------------------------------------------------------
 // Host-side graph: the parsed edge lines, labels masked to CCSRRelSize bits.
 // ---------------------------------------------------------------------------
 struct HostGraph {
     uint32_t n = 0;
-    std::vector<uint32_t> src, dst;   // directed entries, input order
-    std::vector<uint8_t> lab;         // edge label & ((1<<CCSRRelSize)-1)
+    RawVec<uint32_t> src, dst;        // directed entries, input order
+    RawVec<uint8_t> lab;              // edge label & ((1<<CCSRRelSize)-1)
     std::vector<uint32_t> vlabel;     // per vertex id (v lines), 0 if absent
 };
 
@@ -196,7 +222,24 @@ struct gfsm_plan {
 namespace gfsm {
 // host_graph.cpp
 gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGraph &g);
-gfsm_status read_file(const char *path, std::string &out);
+// A file's bytes: mapped read-only where it can be (no copy; the parse
+// threads fault their own chunks in), else read whole into memory.
+class FileBytes {
+public:
+    FileBytes() = default;
+    FileBytes(const FileBytes &) = delete;
+    FileBytes &operator=(const FileBytes &) = delete;
+    ~FileBytes() { close(); }
+    gfsm_status open(const char *path);
+    void close();
+    const char *data() const { return map_ ? static_cast<const char *>(map_) : buf_.data(); }
+    uint64_t size() const { return len_; }
+
+private:
+    void *map_ = nullptr;
+    uint64_t len_ = 0;
+    std::string buf_;
+};
 // weight == nullptr: the reference's matching order.  Otherwise weight[v]
 // estimates query vertex v's data candidates and the order is data-aware
 // (only valid where the count cannot depend on the order).

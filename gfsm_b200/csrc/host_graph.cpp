@@ -5,6 +5,11 @@
 // chunks: the reference reads the file byte by byte on one thread.
 // plan_query restates the reference's matching order and requirement table
 // (HnGPU.cu:749-816 preProcessQuery, ccsr.cpp:98-219).
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -22,17 +27,23 @@ enum LineKind : uint8_t { L_V, L_E, L_END, L_BAD };
 // Tokenises one line the way parseValues does (HnHelper.cuh:233-263): digit
 // runs accumulate into the current value slot with uint32 wrap-around, every
 // other byte moves to the next slot, '\n' ends the line.
+// Every non-digit byte moves to the next slot, so a slot receives at most
+// one digit run: it is accumulated in a register and stored when the run's
+// slot ends.
 inline const char *scan_values(const char *s, const char *end, uint32_t *v, int nv) {
-    uint32_t cur = 0;
+    uint32_t cur = 0, acc = 0;
     for (; s < end; ++s) {
-        char ch = *s;
-        if (ch >= '0' && ch <= '9') {
-            if ((int)cur < nv) v[cur] = v[cur] * 10u + (uint32_t)(ch - '0');
-        } else {
-            ++cur;
-            if (ch == '\n') return s + 1;
+        const uint32_t d = (uint32_t)(uint8_t)*s - (uint32_t)'0';
+        if (d < 10u) {
+            acc = acc * 10u + d;
+            continue;
         }
+        if ((int)cur < nv) v[cur] = acc;
+        acc = 0;
+        ++cur;
+        if (*s == '\n') return s + 1;
     }
+    if ((int)cur < nv) v[cur] = acc;
     return s;
 }
 
@@ -48,56 +59,84 @@ struct ChunkOut {
 };
 
 void scan_chunk(const char *buf, uint64_t b, uint64_t e, uint64_t len, ChunkOut &o) {
-    const char *end = buf + len;
-    uint64_t pos = b;
-    while (pos < e) {
-        const char *line = buf + pos;
-        char ch = *line;
-        const char *nl = static_cast<const char *>(memchr(line, '\n', len - pos));
-        const char *lend = nl ? nl + 1 : end;
+    const char *end = buf + len, *s = buf + b, *const stop = buf + e;
+    {
+        // room for the chunk's lines at the mean length of its first 64 KiB
+        const char *probe = s + std::min<uint64_t>(e - b, 1u << 16);
+        uint64_t lines = 1;
+        for (const char *x = s; x < probe; ++x) lines += *x == '\n';
+        const uint64_t guess = (e - b) / std::max<uint64_t>(1, (uint64_t)(probe - s) / lines) + 16;
+        o.es.reserve(guess);
+        o.ed.reserve(guess);
+        o.el.reserve(guess);
+    }
+    while (s < stop) {
+        const uint64_t pos = (uint64_t)(s - buf);
+        const char ch = *s;
         if (ch == 't') {
-            bool ok = (uint64_t)(end - line) >= 6 && !strncmp(line, "t # -1", 6);
+            bool ok = (uint64_t)(end - s) >= 6 && !strncmp(s, "t # -1", 6);
             o.first_stop = pos;
             o.stop_kind = ok ? L_END : L_BAD;
             return;
         }
-        if (ch == 'v' || ch == 'e') {
-            uint32_t v[3] = {0, 0, 0};
-            const char *vs = line + 2 < lend ? line + 2 : lend;
-            scan_values(vs, lend, v, 3);
-            if (ch == 'v') {
-                o.vid.push_back(v[0]);
-                o.vlab.push_back(v[1]);
-                o.last_v = pos + 1;
-                if (o.first_e != UINT64_MAX && o.first_v_after_e == UINT64_MAX) o.first_v_after_e = pos;
-            } else {
-                if (o.first_e == UINT64_MAX) o.first_e = pos;
-                o.es.push_back(v[0]);
-                o.ed.push_back(v[1]);
-                o.el.push_back(v[2]);
-            }
-        } else {
+        if (ch != 'v' && ch != 'e') {
             o.first_stop = pos;
             o.stop_kind = L_BAD;
             return;
         }
-        pos = (uint64_t)(lend - buf);
+        // the values start two bytes in ("e " / "v "); a line that ends
+        // sooner has none
+        uint32_t v[3] = {0, 0, 0};
+        if (s + 1 >= end) s = end;
+        else if (s[1] == '\n') s += 2;
+        else s = scan_values(s + 2, end, v, 3);
+        if (ch == 'v') {
+            o.vid.push_back(v[0]);
+            o.vlab.push_back(v[1]);
+            o.last_v = pos + 1;
+            if (o.first_e != UINT64_MAX && o.first_v_after_e == UINT64_MAX) o.first_v_after_e = pos;
+        } else {
+            if (o.first_e == UINT64_MAX) o.first_e = pos;
+            o.es.push_back(v[0]);
+            o.ed.push_back(v[1]);
+            o.el.push_back(v[2]);
+        }
     }
 }
 
 }  // namespace
 
-gfsm_status read_file(const char *path, std::string &out) {
-    FILE *f = fopen(path, "rb");
-    if (!f) return GFSM_ERR_MISSING_FILE;  // HnHelper.cuh:289-294
-    fseek(f, 0, SEEK_END);
-    long sz = ftell(f);
-    rewind(f);
-    out.resize(sz > 0 ? (size_t)sz : 0);
-    size_t got = sz > 0 ? fread(&out[0], 1, (size_t)sz, f) : 0;
-    fclose(f);
-    out.resize(got);
+gfsm_status FileBytes::open(const char *path) {
+    close();
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return GFSM_ERR_MISSING_FILE;  // HnHelper.cuh:289-294
+    struct stat sb {};
+    if (fstat(fd, &sb) == 0 && S_ISREG(sb.st_mode) && sb.st_size > 0) {
+        void *m = mmap(nullptr, (size_t)sb.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (m != MAP_FAILED) {
+            map_ = m;
+            len_ = (uint64_t)sb.st_size;
+            ::close(fd);
+            return GFSM_OK;
+        }
+    }
+    // not mappable (a pipe, a special file): read it whole
+    char tmp[1 << 16];
+    for (;;) {
+        const ssize_t got = ::read(fd, tmp, sizeof(tmp));
+        if (got <= 0) break;
+        buf_.append(tmp, (size_t)got);
+    }
+    ::close(fd);
+    len_ = buf_.size();
     return GFSM_OK;
+}
+
+void FileBytes::close() {
+    if (map_) munmap(map_, (size_t)len_);
+    map_ = nullptr;
+    buf_.clear();
+    len_ = 0;
 }
 
 gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGraph &g) {
@@ -131,8 +170,9 @@ gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGra
     std::vector<ChunkOut> outs(nt);
     {
         std::vector<std::thread> th;
-        for (unsigned t = 0; t < nt; ++t)
+        for (unsigned t = 1; t < nt; ++t)
             th.emplace_back([&, t] { scan_chunk(buf, cut[t], cut[t + 1], len, outs[t]); });
+        scan_chunk(buf, cut[0], cut[1], len, outs[0]);
         for (auto &x : th) x.join();
     }
     // Sequential semantics: the parse stops at the first 't' line or bad
@@ -164,19 +204,37 @@ gfsm_status parse_text(const char *buf, uint64_t len, uint32_t rel_bits, HostGra
     g.dst.resize(ne);
     g.lab.resize(ne);
     const uint32_t vert_bits = 32u - rel_bits;
-    uint64_t w = 0;
-    for (unsigned t = 0; t <= last; ++t) {
+    // each chunk's edges go to their place on its own thread; the vertex
+    // lines are applied in file order (a repeated id keeps its last label)
+    std::vector<uint64_t> eoff(last + 2, 0);
+    for (unsigned t = 0; t <= last; ++t) eoff[t + 1] = eoff[t] + outs[t].es.size();
+    std::atomic<bool> oob{false};
+    auto place = [&](unsigned t) {
         const ChunkOut &o = outs[t];
-        for (size_t i = 0; i < o.vid.size(); ++i)
-            if (o.vid[i] < n) g.vlabel[o.vid[i]] = o.vlab[i];
-        for (size_t i = 0; i < o.es.size(); ++i, ++w) {
-            if (o.es[i] >= n || o.ed[i] >= n) return GFSM_ERR_INVALID_DATA;  // reference: out of bounds
-            g.src[w] = o.es[i];
-            g.dst[w] = o.ed[i];
+        const uint64_t w0 = eoff[t];
+        for (size_t i = 0; i < o.es.size(); ++i) {
+            if (o.es[i] >= n || o.ed[i] >= n) {  // reference: out of bounds
+                oob.store(true, std::memory_order_relaxed);
+                return;
+            }
+            g.src[w0 + i] = o.es[i];
+            g.dst[w0 + i] = o.ed[i];
             // (label << CCSRVertSize) keeps the low CCSRRelSize bits (:376)
-            g.lab[w] = (uint8_t)(((uint32_t)(o.el[i] << vert_bits)) >> vert_bits);
+            g.lab[w0 + i] = (uint8_t)(((uint32_t)(o.el[i] << vert_bits)) >> vert_bits);
         }
+    };
+    {
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t <= last; ++t) th.emplace_back(place, t);
+        place(0);
+        for (unsigned t = 0; t <= last; ++t) {
+            const ChunkOut &o = outs[t];
+            for (size_t i = 0; i < o.vid.size(); ++i)
+                if (o.vid[i] < n) g.vlabel[o.vid[i]] = o.vlab[i];
+        }
+        for (auto &x : th) x.join();
     }
+    if (oob.load()) return GFSM_ERR_INVALID_DATA;
     return GFSM_OK;
 }
 
