@@ -129,7 +129,10 @@ const char *gfsm_last_error(gfsm_ctx *ctx);
 
 /* --- graphs ------------------------------------------------------------ */
 /* replaces fileParse (HnHelper.cuh:283-499): parses `t # / v / e` text on the
- * host (multi-threaded) and, for data graphs, builds the CCSR on the device. */
+ * host (multi-threaded) and, for data graphs, builds the CCSR on the device.
+ * A regular file is mapped read-only while it is parsed, not copied: another
+ * process truncating it meanwhile faults this one (SIGBUS), as with any
+ * mapping. */
 gfsm_status gfsm_graph_load_text(gfsm_ctx *ctx, const char *path, gfsm_graph **out);
 gfsm_status gfsm_graph_load_buffer(gfsm_ctx *ctx, const char *buf, uint64_t len, gfsm_graph **out);
 /* Directed edge list (give both directions for an undirected graph).
