@@ -422,8 +422,8 @@ gfsm_status gfsm_query_prepare_batch(gfsm_ctx *ctx, int nq, const uint32_t *nv, 
     const int hw = std::max(1u, std::thread::hardware_concurrency());
     const int nt = std::max(1, std::min(hw, (nq + 63) / 64));
     auto work = [&](int t) {
+        HostGraph h;  // reused: every field is reassigned per query, its capacity kept
         for (int i = t; i < nq; i += nt) {
-            HostGraph h;
             const uint64_t e0 = eoff[i], m = eoff[i + 1] - e0;
             rc[i] = edges_to_host(nv[i], m, src + e0, dst + e0, elabel ? elabel + e0 : nullptr,
                                   vlabel ? vlabel + voff[i] : nullptr, rel_bits, h);
