@@ -145,6 +145,30 @@ def test_parser_error_codes(host_ctx, tmp_path):
     assert ei.value.status == 232
 
 
+def test_file_parse_from_a_pipe_and_an_empty_file(host_ctx, tmp_path):
+    """A regular file is mapped while it is parsed; what cannot be mapped (a
+    named pipe) is read whole instead -- the same graph either way.  An empty
+    file is invalid data, as for the reference (no "t # 0" line)."""
+    import threading
+    text = open(os.path.join(GOLD, "data", "er200.g"), "rb").read()
+    want = host_ctx.file_parse(os.path.join(GOLD, "data", "er200.g")).info()
+    fifo = tmp_path / "pipe.g"
+    os.mkfifo(fifo)
+
+    def write():
+        with open(fifo, "wb") as f:
+            f.write(text)
+    writer = threading.Thread(target=write)
+    writer.start()
+    got = host_ctx.file_parse(str(fifo)).info()
+    writer.join()
+    assert got == want and got["m"] > 0
+    (tmp_path / "empty.g").write_bytes(b"")
+    with pytest.raises(gfsm_b200.GFSMError) as ei:
+        host_ctx.file_parse(str(tmp_path / "empty.g"))
+    assert ei.value.status == 233
+
+
 def test_parser_large_multichunk_matches_oracle(host_ctx, tmp_path):
     """A file big enough to be split across threads parses to the same edges."""
     from gfsm_b200 import synth
