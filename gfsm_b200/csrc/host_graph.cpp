@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
 #include <cstdio>
 #include <cstring>
 #include <thread>
@@ -124,6 +125,7 @@ gfsm_status FileBytes::open(const char *path) {
     char tmp[1 << 16];
     for (;;) {
         const ssize_t got = ::read(fd, tmp, sizeof(tmp));
+        if (got < 0 && errno == EINTR) continue;
         if (got <= 0) break;
         buf_.append(tmp, (size_t)got);
     }
