@@ -248,13 +248,15 @@ def test_batch_planning_reports_the_failing_query(host_ctx):
     assert len(host_ctx.prepare_queries([])) == 0
 
 
-def test_flat_batch_planning_and_plan_batch(host_ctx):
+@pytest.mark.parametrize("nq", [50, 3000])
+def test_flat_batch_planning_and_plan_batch(host_ctx, nq):
     """prepare_queries_flat over flat arrays gives the per-query plans; a
-    PlanBatch indexes as Plan views and closes every plan once."""
+    PlanBatch indexes as Plan views and closes every plan once.  3,000
+    queries plan and free on several host threads."""
     from gfsm_b200 import synth
     g = synth.grid(30, 0.05, 0.02, seed=2)
     g.vlabel = synth.vlabels(g.n, 3, 0.0, seed=4)
-    qs = [synth.rw_query(g, 3 + i % 6, seed=300 + i)[0] for i in range(50)]
+    qs = [synth.rw_query(g, 3 + i % 6, seed=300 + i)[0] for i in range(nq)]
     dirs = [q.directed() for q in qs]
     nv = np.array([q.n for q in qs], np.uint32)
     eoff = np.zeros(len(qs) + 1, np.uint64)
@@ -268,6 +270,7 @@ def test_flat_batch_planning_and_plan_batch(host_ctx):
         one = host_ctx.pre_process_query(host_ctx.graph_from_edges(q.n, a, b, None, q.vlabel))
         assert p.tables()["order"].tolist() == one.tables()["order"].tolist()
         assert p.tables()["reqs"].tolist() == one.tables()["reqs"].tolist()
+        assert p.symmetry() == one.symmetry()
         p.close()  # a view: does not destroy the batch's plan
     assert batch[-1].tables()["k"] == qs[-1].n
     batch.close()
